@@ -1,0 +1,201 @@
+/*
+ * mlbm.h -- C ABI of the B200 D3Q19 Shan-Chen multiphase LBM library
+ * (libmlbm.so).  Plain pointers, sizes and status codes; no C++ or torch types.
+ *
+ * One handle (mlbm_lattice) is one porous domain resident on one GPU.  The
+ * calls map onto the reference's host<->device boundary
+ * (include/iteration_host.h:30-60, src/iteration_host.cu:16-81 of
+ * Amber1995/multiphase_LBM):
+ *
+ *   reference                              this ABI
+ *   ------------------------------------   -----------------------------------
+ *   transfer_parameter(...)                mlbm_set_params
+ *     include/iteration_host.h:30-41
+ *   multiphaselbm_initialization(...)      mlbm_upload_fluid_mask +
+ *     include/iteration_host.h:43-49         mlbm_upload_rho + mlbm_initialize
+ *   multiphaselbm_iteration(step, ...)     mlbm_iterate (n steps per call)
+ *     include/iteration_host.h:56-57
+ *   host reads of managed rho/pressure     mlbm_download_field
+ *     src/multiphase_lbm.cu:249-252
+ *   calc_cluster phase statistics          mlbm_phase_stats
+ *     src/multiphase_lbm.cu:240-316
+ *
+ * Differences from the reference boundary, all deliberate:
+ *   - lattice sizes are runtime arguments (the reference compiles them in,
+ *     include/lbm_model.cuh:4-6);
+ *   - every call returns an mlbm_status instead of exit()ing
+ *     (include/iteration_host.h:6-15); mlbm_last_error() has the message;
+ *   - fields are copied in and out in the reference's [x][y][z] layout
+ *     (z fastest) instead of being shared as managed memory, so a host read
+ *     never races a running kernel.
+ * The three reference entry points themselves, with their own signatures,
+ * are in mlbm_compat.h.
+ */
+#ifndef MLBM_H_
+#define MLBM_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MLBM_ABI_VERSION 1
+
+typedef enum mlbm_status {
+  MLBM_OK = 0,
+  MLBM_ERR_ARG = 1,      /* invalid argument (null, size, enum) */
+  MLBM_ERR_CUDA = 2,     /* CUDA runtime error or no usable device */
+  MLBM_ERR_NOMEM = 3,    /* device allocation refused */
+  MLBM_ERR_STATE = 4,    /* call out of order (e.g. iterate before init) */
+  MLBM_ERR_TIMEOUT = 5,  /* a bounded device wait ran out */
+  MLBM_ERR_IO = 6,       /* file could not be read or written */
+  MLBM_ERR_PARSE = 7     /* malformed input file */
+} mlbm_status;
+
+/* Population storage format. */
+typedef enum mlbm_storage {
+  MLBM_STORE_F32 = 0, /* float populations, float arithmetic (the drop-in) */
+  MLBM_STORE_F16 = 1, /* half(f_i - t_i * rho_shift), float arithmetic */
+  MLBM_STORE_F64 = 2  /* double populations and arithmetic (FP64 oracle) */
+} mlbm_storage;
+
+/* Fields for mlbm_download_field (reference layout [x][y][z], z fastest). */
+typedef enum mlbm_field {
+  MLBM_FIELD_RHO = 0,      /* density (fluid: last step's rho; solid: rhos) */
+  MLBM_FIELD_PRESSURE = 1, /* EOS pressure of rho */
+  MLBM_FIELD_PSI = 2,      /* pseudopotential psi(rho) */
+  MLBM_FIELD_VELOCITY = 3, /* u = (sum f e + tau F)/rho, [x][y][z][3]; written
+                              by the last step of an mlbm_iterate call made
+                              with MLBM_ITER_WRITE_VELOCITY */
+  MLBM_FIELD_POPULATIONS = 4, /* post-collision f*, [x][y][z][19] */
+  MLBM_FIELD_FLUID = 5        /* solid mask as uint8 (1 = fluid) */
+} mlbm_field;
+
+typedef enum mlbm_dtype { MLBM_DTYPE_F32 = 0, MLBM_DTYPE_F64 = 1,
+                          MLBM_DTYPE_U8 = 2 } mlbm_dtype;
+
+/* Flags for mlbm_iterate. */
+#define MLBM_ITER_WRITE_VELOCITY 1u
+
+/* Physics parameters: the arguments of the reference's transfer_parameter
+ * (include/iteration_host.h:30-41, defaults src/multiphase_lbm.cu:35-80) plus
+ * the drainage boundary, which the reference does not have: fluid nodes with
+ * x < inlet_width are held at rho_inlet and fluid nodes with
+ * x >= lx - outlet_width at rho_outlet (density fixed, post-collision
+ * populations the rest equilibrium t_i * rho).  Both widths 0 = periodic. */
+typedef struct mlbm_params {
+  float tau;
+  float G;
+  float T_Tc;
+  float rhol_spinodal;
+  float rhog_spinodal;
+  float rho_increment;
+  float rhos;
+  float inject_position;
+  int32_t carn_star;
+  int32_t inject_density;
+  uint64_t rho_inject_period; /* 0 = never inject */
+  uint64_t stat_period;
+  int32_t inlet_width;
+  int32_t outlet_width;
+  float rho_inlet;
+  float rho_outlet;
+  float rho_shift; /* FP16 storage only: populations stored minus t_i*rho_shift */
+  int32_t reserved;
+} mlbm_params;
+
+/* Phase statistics over fluid nodes (calc_cluster, src/multiphase_lbm.cu:
+ * 240-316; min/max of write_stats, :1057-1072).  Liquid: rho > rhol_spinodal;
+ * vapour: rho < rhog_spinodal.  Sums and averages are accumulated in FP64. */
+typedef struct mlbm_stats {
+  int64_t n_fluid;
+  int64_t n_liquid;
+  int64_t n_vapour;
+  int64_t n_liquid_solid_boundary;
+  int64_t n_liquid_vapour_boundary;
+  double mass; /* sum of rho over fluid nodes */
+  double sum_p_liquid, sum_p_vapour, sum_rho_liquid, sum_rho_vapour;
+  double saturation;
+  double avg_p_liquid, avg_p_vapour, suction;
+  double avg_rho_liquid, avg_rho_vapour;
+  double ratio_liquid_solid_boundary, ratio_liquid_vapour_boundary;
+  double min_rho, max_rho, min_p, max_p;
+} mlbm_stats;
+
+typedef struct mlbm_lattice mlbm_lattice;
+
+/* Library version / diagnostics. */
+int32_t mlbm_abi_version(void);
+const char* mlbm_status_string(int32_t status);
+/* Message of the last failing call on this host thread ("" if none). */
+const char* mlbm_last_error(void);
+/* D3Q19 tables as the kernels use them: e[19*3] (ex,ey,ez per direction),
+ * w[19] (include/lbm_model.cuh:35-54). */
+void mlbm_d3q19(int32_t* e, float* w);
+
+/* Create a lattice of lx*ly*lz nodes on `device` with the given storage.
+ * Allocates all device memory up front (MLBM_ERR_NOMEM if refused). */
+mlbm_status mlbm_lattice_create(int32_t lx, int32_t ly, int32_t lz,
+                                int32_t storage, int32_t device,
+                                mlbm_lattice** out);
+mlbm_status mlbm_lattice_destroy(mlbm_lattice* lat);
+/* Device bytes held by a lattice of this size and storage (no allocation). */
+uint64_t mlbm_lattice_bytes(int32_t lx, int32_t ly, int32_t lz,
+                            int32_t storage);
+
+/* CUDA stream (cudaStream_t) the lattice's work is issued on; NULL = the
+ * legacy default stream. */
+mlbm_status mlbm_set_stream(mlbm_lattice* lat, void* stream);
+
+/* transfer_parameter */
+mlbm_status mlbm_set_params(mlbm_lattice* lat, const mlbm_params* p);
+
+/* Geometry and initial density, host arrays in the reference layout
+ * [x][y][z] (z fastest): is_fluid (nonzero = fluid) and rho (float). */
+mlbm_status mlbm_upload_fluid_mask(mlbm_lattice* lat, const uint8_t* is_fluid);
+mlbm_status mlbm_upload_rho(mlbm_lattice* lat, const float* rho);
+/* Same, from device memory (same layout). */
+mlbm_status mlbm_upload_fluid_mask_device(mlbm_lattice* lat,
+                                          const uint8_t* is_fluid_dev);
+mlbm_status mlbm_upload_rho_device(mlbm_lattice* lat, const float* rho_dev);
+
+/* multiphaselbm_initialization: f_i = t_i rho everywhere, solids take
+ * rho = rhos (include/iteration_kernel.cuh:9-29).  Needs params, mask, rho. */
+mlbm_status mlbm_initialize(mlbm_lattice* lat);
+
+/* multiphaselbm_iteration for steps step0 .. step0+nsteps-1 (streaming,
+ * bounce-back, Shan-Chen force, velocity shift, BGK).  Asynchronous on the
+ * lattice's stream. */
+mlbm_status mlbm_iterate(mlbm_lattice* lat, int64_t step0, int32_t nsteps,
+                         int32_t reverse, uint32_t inject_type,
+                         uint32_t flags);
+
+/* Copy a field out in the reference layout.  dtype: MLBM_DTYPE_F32 or
+ * MLBM_DTYPE_F64 (F64 keeps an FP64 lattice's full precision), U8 for
+ * MLBM_FIELD_FLUID.  host_out: lx*ly*lz*components elements.  Synchronous. */
+mlbm_status mlbm_download_field(mlbm_lattice* lat, int32_t field,
+                                int32_t dtype, void* host_out);
+/* Same into device memory (stream-ordered, no synchronisation). */
+mlbm_status mlbm_download_field_device(mlbm_lattice* lat, int32_t field,
+                                       int32_t dtype, void* dev_out);
+
+/* Phase statistics of the current state (device reduction, deterministic).
+ * Synchronous. */
+mlbm_status mlbm_phase_stats(mlbm_lattice* lat, mlbm_stats* out);
+/* Per-x-plane counts of fluid and liquid nodes (int64[lx] each).  Sync. */
+mlbm_status mlbm_plane_profile(mlbm_lattice* lat, int64_t* n_fluid_x,
+                               int64_t* n_liquid_x);
+
+/* Information about the lattice: dims[3], storage, phase of the stored
+ * state (0/1, see kernels), initialised flag. */
+mlbm_status mlbm_lattice_info(const mlbm_lattice* lat, int32_t* dims,
+                              int32_t* storage, int32_t* phase,
+                              int32_t* initialized);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MLBM_H_ */

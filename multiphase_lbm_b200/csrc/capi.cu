@@ -1,0 +1,595 @@
+// capi.cu -- implementation of the C ABI in include/mlbm.h.
+//
+// Owns the device memory of each lattice and issues the kernels of
+// kernels.cuh / io_kernels.cuh on the lattice's stream.  Host-side errors are
+// returned as mlbm_status with a message kept per host thread; nothing here
+// exits or falls back to the CPU.
+#include <cuda_runtime.h>
+
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+
+#include "../../include/mlbm.h"
+#include "capi_internal.h"
+#include "io_kernels.cuh"
+#include "kernels.cuh"
+
+using namespace mlbm;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+mlbm_status fail(mlbm_status st, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  g_last_error = buf;
+  return st;
+}
+
+}  // namespace
+
+namespace mlbm {
+
+mlbm_status set_error(mlbm_status st, const char* msg) {
+  g_last_error = msg;
+  return st;
+}
+
+mlbm_status cuda_fail(cudaError_t e, const char* where) {
+  if (e == cudaErrorMemoryAllocation)
+    return fail(MLBM_ERR_NOMEM, "%s: %s", where, cudaGetErrorString(e));
+  return fail(MLBM_ERR_CUDA, "%s: %s", where, cudaGetErrorString(e));
+}
+
+size_t pop_elem_bytes(int storage) {
+  return storage == MLBM_STORE_F16 ? 2 : (storage == MLBM_STORE_F64 ? 8 : 4);
+}
+size_t real_bytes(int storage) { return storage == MLBM_STORE_F64 ? 8 : 4; }
+
+Geom make_geom(int lx, int ly, int lz) {
+  Geom g;
+  g.lx = lx;
+  g.ly = ly;
+  g.lz = lz;
+  g.px = (lx + 31) / 32 * 32;
+  g.wpr = g.px / 32;
+  g.plane = (long long)lz * ly * g.px;
+  return g;
+}
+
+}  // namespace mlbm
+
+#define CUDA_TRY(expr, where)                           \
+  do {                                                  \
+    cudaError_t _e = (expr);                            \
+    if (_e != cudaSuccess) return mlbm::cuda_fail(_e, where); \
+  } while (0)
+
+namespace {
+
+dim3 node_block() { return dim3(32, 4, 1); }
+dim3 node_grid(const Geom& g) {
+  return dim3(g.px / 32, (g.ly + 3) / 4, g.lz);
+}
+
+Phys to_phys(const mlbm_params& p) {
+  Phys q;
+  q.tau = p.tau;
+  q.G = p.G;
+  q.T_Tc = p.T_Tc;
+  q.rhol_spinodal = p.rhol_spinodal;
+  q.rhog_spinodal = p.rhog_spinodal;
+  q.rhos = p.rhos;
+  q.rho_increment = p.rho_increment;
+  q.inject_position = p.inject_position;
+  q.carn_star = p.carn_star;
+  q.rho_inject_period = p.rho_inject_period;
+  q.inlet_width = p.inlet_width;
+  q.outlet_width = p.outlet_width;
+  q.rho_inlet = p.rho_inlet;
+  q.rho_outlet = p.rho_outlet;
+  q.rho_shift = p.rho_shift;
+  return q;
+}
+
+mlbm_status check_lat(const mlbm_lattice* lat) {
+  if (!lat) return fail(MLBM_ERR_ARG, "null lattice handle");
+  return MLBM_OK;
+}
+
+mlbm_status activate(const mlbm_lattice* lat) {
+  CUDA_TRY(cudaSetDevice(lat->device), "cudaSetDevice");
+  return MLBM_OK;
+}
+
+template <typename T>
+mlbm_status launch_steps(mlbm_lattice* lat, int64_t step0, int32_t nsteps,
+                         int32_t reverse, uint32_t inject_type,
+                         uint32_t flags) {
+  using R = typename Pop<T>::Real;
+  T* pop = static_cast<T*>(lat->pop);
+  R* rho = static_cast<R*>(lat->rho);
+  R* psi = static_cast<R*>(lat->psi);
+  const dim3 grid = node_grid(lat->g), block = node_block();
+  for (int32_t s = 0; s < nsteps; ++s) {
+    StepArgs a{(long long)(step0 + s), reverse, inject_type};
+    const bool wu = (flags & MLBM_ITER_WRITE_VELOCITY) && s == nsteps - 1;
+    if (lat->phase == 0) {
+      k_density<T, 0><<<grid, block, 0, lat->stream>>>(pop, lat->mask, rho, psi,
+                                                       lat->g, lat->phys, a);
+      if (wu)
+        k_update<T, 0, true><<<grid, block, 0, lat->stream>>>(
+            pop, lat->mask, rho, psi, lat->vel, lat->g, lat->phys, a);
+      else
+        k_update<T, 0, false><<<grid, block, 0, lat->stream>>>(
+            pop, lat->mask, rho, psi, lat->vel, lat->g, lat->phys, a);
+    } else {
+      k_density<T, 1><<<grid, block, 0, lat->stream>>>(pop, lat->mask, rho, psi,
+                                                       lat->g, lat->phys, a);
+      if (wu)
+        k_update<T, 1, true><<<grid, block, 0, lat->stream>>>(
+            pop, lat->mask, rho, psi, lat->vel, lat->g, lat->phys, a);
+      else
+        k_update<T, 1, false><<<grid, block, 0, lat->stream>>>(
+            pop, lat->mask, rho, psi, lat->vel, lat->g, lat->phys, a);
+    }
+    lat->phase ^= 1;
+    if (wu) lat->vel_valid = true;
+  }
+  CUDA_TRY(cudaGetLastError(), "time-step launch");
+  return MLBM_OK;
+}
+
+template <typename T>
+mlbm_status launch_init(mlbm_lattice* lat) {
+  using R = typename Pop<T>::Real;
+  k_init<T><<<node_grid(lat->g), node_block(), 0, lat->stream>>>(
+      static_cast<T*>(lat->pop), lat->mask, lat->rho_init,
+      static_cast<R*>(lat->rho), static_cast<R*>(lat->psi), lat->g, lat->phys);
+  CUDA_TRY(cudaGetLastError(), "init launch");
+  return MLBM_OK;
+}
+
+template <typename T, typename O>
+void launch_pop_out(mlbm_lattice* lat, O* out) {
+  k_pop_to_ref<T, O><<<node_grid(lat->g), node_block(), 0, lat->stream>>>(
+      static_cast<const T*>(lat->pop), lat->mask, out, lat->g, lat->phys,
+      lat->phase);
+}
+
+template <typename R, typename O>
+void launch_scalar_out(mlbm_lattice* lat, int field, O* out) {
+  k_scalar_to_ref<R, O><<<node_grid(lat->g), node_block(), 0, lat->stream>>>(
+      static_cast<const R*>(lat->rho), lat->mask, out, lat->g, lat->phys,
+      field);
+}
+
+template <typename O>
+mlbm_status field_out(mlbm_lattice* lat, int32_t field, O* dev_out) {
+  switch (field) {
+    case MLBM_FIELD_RHO:
+    case MLBM_FIELD_PRESSURE:
+    case MLBM_FIELD_PSI:
+      if (lat->storage == MLBM_STORE_F64)
+        launch_scalar_out<double, O>(lat, field, dev_out);
+      else
+        launch_scalar_out<float, O>(lat, field, dev_out);
+      break;
+    case MLBM_FIELD_VELOCITY:
+      if (!lat->vel_valid)
+        return fail(MLBM_ERR_STATE,
+                    "velocity not written: iterate with "
+                    "MLBM_ITER_WRITE_VELOCITY first");
+      k_vel_to_ref<O><<<node_grid(lat->g), node_block(), 0, lat->stream>>>(
+          lat->vel, dev_out, lat->g);
+      break;
+    case MLBM_FIELD_POPULATIONS:
+      if (lat->storage == MLBM_STORE_F32)
+        launch_pop_out<float, O>(lat, dev_out);
+      else if (lat->storage == MLBM_STORE_F16)
+        launch_pop_out<__half, O>(lat, dev_out);
+      else
+        launch_pop_out<double, O>(lat, dev_out);
+      break;
+    default:
+      return fail(MLBM_ERR_ARG, "unknown field %d", field);
+  }
+  CUDA_TRY(cudaGetLastError(), "field download launch");
+  return MLBM_OK;
+}
+
+size_t field_components(int32_t field) {
+  return field == MLBM_FIELD_VELOCITY ? 3
+         : field == MLBM_FIELD_POPULATIONS ? Q
+                                           : 1;
+}
+
+mlbm_status ensure_staging(mlbm_lattice* lat, size_t bytes) {
+  if (lat->staging_bytes >= bytes) return MLBM_OK;
+  if (lat->staging) cudaFree(lat->staging);
+  lat->staging = nullptr;
+  lat->staging_bytes = 0;
+  CUDA_TRY(cudaMalloc(&lat->staging, bytes), "staging allocation");
+  lat->staging_bytes = bytes;
+  return MLBM_OK;
+}
+
+}  // namespace
+
+// ============================================================================
+extern "C" {
+
+int32_t mlbm_abi_version(void) { return MLBM_ABI_VERSION; }
+
+const char* mlbm_status_string(int32_t s) {
+  switch (s) {
+    case MLBM_OK: return "ok";
+    case MLBM_ERR_ARG: return "invalid argument";
+    case MLBM_ERR_CUDA: return "CUDA error";
+    case MLBM_ERR_NOMEM: return "out of device memory";
+    case MLBM_ERR_STATE: return "call out of order";
+    case MLBM_ERR_TIMEOUT: return "device wait timed out";
+    case MLBM_ERR_IO: return "I/O error";
+    case MLBM_ERR_PARSE: return "parse error";
+  }
+  return "unknown status";
+}
+
+const char* mlbm_last_error(void) { return g_last_error.c_str(); }
+
+void mlbm_d3q19(int32_t* e, float* w) {
+  for (int i = 0; i < Q; ++i) {
+    if (e) {
+      e[3 * i] = ex(i);
+      e[3 * i + 1] = ey(i);
+      e[3 * i + 2] = ez(i);
+    }
+    if (w) w[i] = weight<float>(i);
+  }
+}
+
+uint64_t mlbm_lattice_bytes(int32_t lx, int32_t ly, int32_t lz,
+                            int32_t storage) {
+  if (lx <= 0 || ly <= 0 || lz <= 0) return 0;
+  const Geom g = make_geom(lx, ly, lz);
+  const uint64_t np = (uint64_t)g.plane;
+  return np * Q * pop_elem_bytes(storage)     // populations
+         + 2 * np * real_bytes(storage)       // rho, psi
+         + np * 4                             // initial density
+         + (uint64_t)g.lz * g.ly * g.wpr * 4  // mask
+         + np * 12;                           // velocity
+}
+
+mlbm_status mlbm_lattice_create(int32_t lx, int32_t ly, int32_t lz,
+                                int32_t storage, int32_t device,
+                                mlbm_lattice** out) {
+  if (!out) return fail(MLBM_ERR_ARG, "null output pointer");
+  *out = nullptr;
+  if (lx < 1 || ly < 1 || lz < 1 || lz > 65535 || ly > (1 << 24) ||
+      lx > (1 << 24))
+    return fail(MLBM_ERR_ARG, "invalid lattice size %d x %d x %d", lx, ly, lz);
+  if (storage < MLBM_STORE_F32 || storage > MLBM_STORE_F64)
+    return fail(MLBM_ERR_ARG, "invalid storage %d", storage);
+  int ndev = 0;
+  CUDA_TRY(cudaGetDeviceCount(&ndev), "cudaGetDeviceCount");
+  if (device < 0 || device >= ndev)
+    return fail(MLBM_ERR_CUDA, "device %d not available (%d devices)", device,
+                ndev);
+  CUDA_TRY(cudaSetDevice(device), "cudaSetDevice");
+  mlbm_lattice* lat = new (std::nothrow) mlbm_lattice();
+  if (!lat) return fail(MLBM_ERR_NOMEM, "host allocation failed");
+  lat->device = device;
+  lat->storage = storage;
+  lat->g = make_geom(lx, ly, lz);
+  const size_t np = (size_t)lat->g.plane;
+  const size_t mask_words = (size_t)lz * ly * lat->g.wpr;
+  cudaError_t e = cudaSuccess;
+  auto alloc = [&](void** p, size_t bytes) {
+    if (e == cudaSuccess) e = cudaMalloc(p, bytes);
+  };
+  alloc(&lat->pop, np * Q * pop_elem_bytes(storage));
+  alloc(&lat->rho, np * real_bytes(storage));
+  alloc(&lat->psi, np * real_bytes(storage));
+  alloc((void**)&lat->rho_init, np * sizeof(float));
+  alloc((void**)&lat->mask, mask_words * sizeof(uint32_t));
+  alloc((void**)&lat->vel, np * 3 * sizeof(float));
+  if (e == cudaSuccess) e = cudaMemset(lat->mask, 0, mask_words * 4);
+  if (e == cudaSuccess) e = cudaMemset(lat->rho_init, 0, np * sizeof(float));
+  if (e != cudaSuccess) {
+    mlbm_lattice_destroy(lat);
+    cudaGetLastError();
+    return cuda_fail(e, "lattice allocation");
+  }
+  *out = lat;
+  return MLBM_OK;
+}
+
+mlbm_status mlbm_lattice_destroy(mlbm_lattice* lat) {
+  if (!lat) return MLBM_OK;
+  cudaSetDevice(lat->device);
+  if (lat->stream_owned_sync) cudaStreamSynchronize(lat->stream);
+  cudaFree(lat->pop);
+  cudaFree(lat->rho);
+  cudaFree(lat->psi);
+  cudaFree(lat->rho_init);
+  cudaFree(lat->mask);
+  cudaFree(lat->vel);
+  cudaFree(lat->staging);
+  cudaFree(lat->stats_scratch);
+  delete lat;
+  return MLBM_OK;
+}
+
+mlbm_status mlbm_set_stream(mlbm_lattice* lat, void* stream) {
+  if (mlbm_status st = check_lat(lat)) return st;
+  lat->stream = static_cast<cudaStream_t>(stream);
+  return MLBM_OK;
+}
+
+mlbm_status mlbm_set_params(mlbm_lattice* lat, const mlbm_params* p) {
+  if (mlbm_status st = check_lat(lat)) return st;
+  if (!p) return fail(MLBM_ERR_ARG, "null params");
+  if (!(p->tau > 0.f)) return fail(MLBM_ERR_ARG, "tau must be > 0 (got %g)", p->tau);
+  if (p->inlet_width < 0 || p->outlet_width < 0 ||
+      p->inlet_width + p->outlet_width > lat->g.lx)
+    return fail(MLBM_ERR_ARG, "invalid drainage slab widths %d, %d",
+                p->inlet_width, p->outlet_width);
+  if (p->carn_star && p->G == 0.f)
+    return fail(MLBM_ERR_ARG, "Carnahan-Starling psi needs G != 0");
+  lat->params = *p;
+  lat->phys = to_phys(*p);
+  lat->has_params = true;
+  return MLBM_OK;
+}
+
+static mlbm_status upload_mask_impl(mlbm_lattice* lat, const uint8_t* src,
+                                    cudaMemcpyKind kind) {
+  const Geom& g = lat->g;
+  const size_t n = (size_t)g.lx * g.ly * g.lz;
+  if (mlbm_status st = ensure_staging(lat, n)) return st;
+  CUDA_TRY(cudaMemcpyAsync(lat->staging, src, n, kind, lat->stream),
+           "mask upload copy");
+  k_pack_mask<<<node_grid(g), node_block(), 0, lat->stream>>>(
+      static_cast<const uint8_t*>(lat->staging), lat->mask, g);
+  CUDA_TRY(cudaGetLastError(), "mask pack launch");
+  CUDA_TRY(cudaStreamSynchronize(lat->stream), "mask upload");
+  lat->has_mask = true;
+  lat->initialized = false;
+  return MLBM_OK;
+}
+
+static mlbm_status upload_rho_impl(mlbm_lattice* lat, const float* src,
+                                   cudaMemcpyKind kind) {
+  const Geom& g = lat->g;
+  const size_t n = (size_t)g.lx * g.ly * g.lz;
+  if (mlbm_status st = ensure_staging(lat, n * sizeof(float))) return st;
+  CUDA_TRY(cudaMemcpyAsync(lat->staging, src, n * sizeof(float), kind,
+                           lat->stream),
+           "rho upload copy");
+  k_rho_from_ref<<<node_grid(g), node_block(), 0, lat->stream>>>(
+      static_cast<const float*>(lat->staging), lat->rho_init, g);
+  CUDA_TRY(cudaGetLastError(), "rho transpose launch");
+  CUDA_TRY(cudaStreamSynchronize(lat->stream), "rho upload");
+  lat->has_rho = true;
+  lat->initialized = false;
+  return MLBM_OK;
+}
+
+mlbm_status mlbm_upload_fluid_mask(mlbm_lattice* lat, const uint8_t* f) {
+  if (mlbm_status st = check_lat(lat)) return st;
+  if (!f) return fail(MLBM_ERR_ARG, "null mask");
+  if (mlbm_status st = activate(lat)) return st;
+  return upload_mask_impl(lat, f, cudaMemcpyHostToDevice);
+}
+mlbm_status mlbm_upload_fluid_mask_device(mlbm_lattice* lat, const uint8_t* f) {
+  if (mlbm_status st = check_lat(lat)) return st;
+  if (!f) return fail(MLBM_ERR_ARG, "null mask");
+  if (mlbm_status st = activate(lat)) return st;
+  return upload_mask_impl(lat, f, cudaMemcpyDeviceToDevice);
+}
+mlbm_status mlbm_upload_rho(mlbm_lattice* lat, const float* r) {
+  if (mlbm_status st = check_lat(lat)) return st;
+  if (!r) return fail(MLBM_ERR_ARG, "null rho");
+  if (mlbm_status st = activate(lat)) return st;
+  return upload_rho_impl(lat, r, cudaMemcpyHostToDevice);
+}
+mlbm_status mlbm_upload_rho_device(mlbm_lattice* lat, const float* r) {
+  if (mlbm_status st = check_lat(lat)) return st;
+  if (!r) return fail(MLBM_ERR_ARG, "null rho");
+  if (mlbm_status st = activate(lat)) return st;
+  return upload_rho_impl(lat, r, cudaMemcpyDeviceToDevice);
+}
+
+mlbm_status mlbm_initialize(mlbm_lattice* lat) {
+  if (mlbm_status st = check_lat(lat)) return st;
+  if (!lat->has_params || !lat->has_mask || !lat->has_rho)
+    return fail(MLBM_ERR_STATE,
+                "initialize needs params, fluid mask and rho first");
+  if (mlbm_status st = activate(lat)) return st;
+  mlbm_status st;
+  switch (lat->storage) {
+    case MLBM_STORE_F32: st = launch_init<float>(lat); break;
+    case MLBM_STORE_F16: st = launch_init<__half>(lat); break;
+    default: st = launch_init<double>(lat); break;
+  }
+  if (st) return st;
+  lat->phase = 0;
+  lat->initialized = true;
+  lat->vel_valid = false;
+  return MLBM_OK;
+}
+
+mlbm_status mlbm_iterate(mlbm_lattice* lat, int64_t step0, int32_t nsteps,
+                         int32_t reverse, uint32_t inject_type,
+                         uint32_t flags) {
+  if (mlbm_status st = check_lat(lat)) return st;
+  if (!lat->initialized)
+    return fail(MLBM_ERR_STATE, "iterate before initialize");
+  if (nsteps < 0) return fail(MLBM_ERR_ARG, "negative step count");
+  if (nsteps == 0) return MLBM_OK;
+  if (mlbm_status st = activate(lat)) return st;
+  switch (lat->storage) {
+    case MLBM_STORE_F32:
+      return launch_steps<float>(lat, step0, nsteps, reverse, inject_type, flags);
+    case MLBM_STORE_F16:
+      return launch_steps<__half>(lat, step0, nsteps, reverse, inject_type, flags);
+    default:
+      return launch_steps<double>(lat, step0, nsteps, reverse, inject_type, flags);
+  }
+}
+
+mlbm_status mlbm_download_field_device(mlbm_lattice* lat, int32_t field,
+                                       int32_t dtype, void* dev_out) {
+  if (mlbm_status st = check_lat(lat)) return st;
+  if (!dev_out) return fail(MLBM_ERR_ARG, "null output");
+  if (mlbm_status st = activate(lat)) return st;
+  if (field == MLBM_FIELD_FLUID) {
+    if (dtype != MLBM_DTYPE_U8)
+      return fail(MLBM_ERR_ARG, "the fluid mask downloads as MLBM_DTYPE_U8");
+    k_fluid_to_ref<<<node_grid(lat->g), node_block(), 0, lat->stream>>>(
+        lat->mask, static_cast<uint8_t*>(dev_out), lat->g);
+    CUDA_TRY(cudaGetLastError(), "mask download launch");
+    return MLBM_OK;
+  }
+  if (!lat->initialized)
+    return fail(MLBM_ERR_STATE, "field download before initialize");
+  if (dtype == MLBM_DTYPE_F32)
+    return field_out<float>(lat, field, static_cast<float*>(dev_out));
+  if (dtype == MLBM_DTYPE_F64)
+    return field_out<double>(lat, field, static_cast<double*>(dev_out));
+  return fail(MLBM_ERR_ARG, "invalid dtype %d for field %d", dtype, field);
+}
+
+mlbm_status mlbm_download_field(mlbm_lattice* lat, int32_t field,
+                                int32_t dtype, void* host_out) {
+  if (mlbm_status st = check_lat(lat)) return st;
+  if (!host_out) return fail(MLBM_ERR_ARG, "null output");
+  const Geom& g = lat->g;
+  const size_t esz = dtype == MLBM_DTYPE_F64 ? 8 : (dtype == MLBM_DTYPE_U8 ? 1 : 4);
+  const size_t bytes = (size_t)g.lx * g.ly * g.lz * field_components(field) * esz;
+  if (mlbm_status st = activate(lat)) return st;
+  if (mlbm_status st = ensure_staging(lat, bytes)) return st;
+  if (mlbm_status st = mlbm_download_field_device(lat, field, dtype, lat->staging))
+    return st;
+  CUDA_TRY(cudaMemcpyAsync(host_out, lat->staging, bytes,
+                           cudaMemcpyDeviceToHost, lat->stream),
+           "field download copy");
+  CUDA_TRY(cudaStreamSynchronize(lat->stream), "field download");
+  return MLBM_OK;
+}
+
+mlbm_status mlbm_phase_stats(mlbm_lattice* lat, mlbm_stats* out) {
+  if (mlbm_status st = check_lat(lat)) return st;
+  if (!out) return fail(MLBM_ERR_ARG, "null output");
+  if (!lat->initialized) return fail(MLBM_ERR_STATE, "stats before initialize");
+  if (mlbm_status st = activate(lat)) return st;
+  int nsm = 148;
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, lat->device);
+  const long long total = (long long)lat->g.lx * lat->g.ly * lat->g.lz;
+  int nblocks = (int)std::min<long long>((long long)nsm * 4,
+                                         (total + kStatThreads - 1) / kStatThreads);
+  if (nblocks < 1) nblocks = 1;
+  const size_t need = ((size_t)nblocks + 1) * ST_COUNT * sizeof(double);
+  if (lat->stats_scratch_bytes < need) {
+    cudaFree(lat->stats_scratch);
+    lat->stats_scratch = nullptr;
+    lat->stats_scratch_bytes = 0;
+    CUDA_TRY(cudaMalloc((void**)&lat->stats_scratch, need), "stats scratch");
+    lat->stats_scratch_bytes = need;
+  }
+  double* partial = lat->stats_scratch;
+  double* fin = partial + (size_t)nblocks * ST_COUNT;
+  if (lat->storage == MLBM_STORE_F64)
+    k_stats_partial<double><<<nblocks, kStatThreads, 0, lat->stream>>>(
+        static_cast<const double*>(lat->rho), lat->mask, lat->g, lat->phys,
+        partial);
+  else
+    k_stats_partial<float><<<nblocks, kStatThreads, 0, lat->stream>>>(
+        static_cast<const float*>(lat->rho), lat->mask, lat->g, lat->phys,
+        partial);
+  k_stats_final<<<1, 32, 0, lat->stream>>>(partial, nblocks, fin);
+  CUDA_TRY(cudaGetLastError(), "stats launch");
+  double h[ST_COUNT];
+  CUDA_TRY(cudaMemcpyAsync(h, fin, sizeof h, cudaMemcpyDeviceToHost, lat->stream),
+           "stats copy");
+  CUDA_TRY(cudaStreamSynchronize(lat->stream), "stats");
+  std::memset(out, 0, sizeof *out);
+  out->n_fluid = (int64_t)h[ST_NF];
+  out->n_liquid = (int64_t)h[ST_NL];
+  out->n_vapour = (int64_t)h[ST_NV];
+  out->n_liquid_solid_boundary = (int64_t)h[ST_NLS];
+  out->n_liquid_vapour_boundary = (int64_t)h[ST_NLV];
+  out->mass = h[ST_MASS];
+  out->sum_p_liquid = h[ST_PL];
+  out->sum_p_vapour = h[ST_PV];
+  out->sum_rho_liquid = h[ST_RL];
+  out->sum_rho_vapour = h[ST_RV];
+  out->saturation = out->n_fluid ? h[ST_NL] / h[ST_NF] : 0.0;
+  if (out->n_liquid) {
+    out->avg_p_liquid = h[ST_PL] / h[ST_NL];
+    out->avg_rho_liquid = h[ST_RL] / h[ST_NL];
+    out->ratio_liquid_solid_boundary = h[ST_NLS] / h[ST_NL];
+    out->ratio_liquid_vapour_boundary = h[ST_NLV] / h[ST_NL];
+  }
+  if (out->n_vapour) {
+    out->avg_p_vapour = h[ST_PV] / h[ST_NV];
+    out->avg_rho_vapour = h[ST_RV] / h[ST_NV];
+  }
+  out->suction = out->avg_p_vapour - out->avg_p_liquid;
+  out->min_rho = h[ST_MINR];
+  out->max_rho = h[ST_MAXR];
+  out->min_p = h[ST_MINP];
+  out->max_p = h[ST_MAXP];
+  return MLBM_OK;
+}
+
+mlbm_status mlbm_plane_profile(mlbm_lattice* lat, int64_t* n_fluid_x,
+                               int64_t* n_liquid_x) {
+  if (mlbm_status st = check_lat(lat)) return st;
+  if (!n_fluid_x || !n_liquid_x) return fail(MLBM_ERR_ARG, "null output");
+  if (!lat->initialized) return fail(MLBM_ERR_STATE, "profile before initialize");
+  if (mlbm_status st = activate(lat)) return st;
+  const int lx = lat->g.lx;
+  const size_t bytes = 2 * (size_t)lx * sizeof(unsigned long long);
+  if (mlbm_status st = ensure_staging(lat, bytes)) return st;
+  auto* nf = static_cast<unsigned long long*>(lat->staging);
+  auto* nl = nf + lx;
+  CUDA_TRY(cudaMemsetAsync(nf, 0, bytes, lat->stream), "profile clear");
+  if (lat->storage == MLBM_STORE_F64)
+    k_plane_profile<double><<<node_grid(lat->g), node_block(), 0, lat->stream>>>(
+        static_cast<const double*>(lat->rho), lat->mask, lat->g, lat->phys, nf, nl);
+  else
+    k_plane_profile<float><<<node_grid(lat->g), node_block(), 0, lat->stream>>>(
+        static_cast<const float*>(lat->rho), lat->mask, lat->g, lat->phys, nf, nl);
+  CUDA_TRY(cudaGetLastError(), "profile launch");
+  CUDA_TRY(cudaMemcpyAsync(n_fluid_x, nf, lx * 8, cudaMemcpyDeviceToHost,
+                           lat->stream), "profile copy");
+  CUDA_TRY(cudaMemcpyAsync(n_liquid_x, nl, lx * 8, cudaMemcpyDeviceToHost,
+                           lat->stream), "profile copy");
+  CUDA_TRY(cudaStreamSynchronize(lat->stream), "profile");
+  return MLBM_OK;
+}
+
+mlbm_status mlbm_lattice_info(const mlbm_lattice* lat, int32_t* dims,
+                              int32_t* storage, int32_t* phase,
+                              int32_t* initialized) {
+  if (mlbm_status st = check_lat(lat)) return st;
+  if (dims) {
+    dims[0] = lat->g.lx;
+    dims[1] = lat->g.ly;
+    dims[2] = lat->g.lz;
+  }
+  if (storage) *storage = lat->storage;
+  if (phase) *phase = lat->phase;
+  if (initialized) *initialized = lat->initialized ? 1 : 0;
+  return MLBM_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,215 @@
+// io_kernels.cuh -- layout conversion between the reference's [x][y][z]
+// arrays and the internal structure-of-arrays lattice, and the device
+// reductions behind the phase statistics.
+#pragma once
+
+#include "lattice.cuh"
+
+namespace mlbm {
+
+// Reference layout index: ((x * ly + y) * lz + z), z fastest
+// (include/lbm_model.cuh:18-22).
+__device__ __forceinline__ long long ref_index(const Geom& g, int x, int y,
+                                               int z) {
+  return ((long long)x * g.ly + y) * g.lz + z;
+}
+
+// Internal-layout kernels use blockDim (32, 4) over (x, y) and grid.z = z.
+#define MLBM_NODE_COORDS                              \
+  const int x = blockIdx.x * 32 + threadIdx.x;        \
+  const int y = blockIdx.y * blockDim.y + threadIdx.y; \
+  const int z = blockIdx.z;
+
+// Pack a uint8 [x][y][z] fluid array into the bit mask; every warp covers one
+// aligned 32-node run of a row.
+__global__ void k_pack_mask(const uint8_t* __restrict__ fluid_ref,
+                            uint32_t* __restrict__ mask, Geom g) {
+  MLBM_NODE_COORDS
+  if (y >= g.ly) return;  // whole warp exits together (warp = one row run)
+  const bool f = (x < g.lx) && fluid_ref[ref_index(g, x, y, z)] != 0;
+  const uint32_t w = __ballot_sync(0xffffffffu, f);
+  if ((threadIdx.x & 31) == 0)
+    mask[((long long)z * g.ly + y) * g.wpr + (x >> 5)] = w;
+}
+
+__global__ void k_rho_from_ref(const float* __restrict__ rho_ref,
+                               float* __restrict__ rho_int, Geom g) {
+  MLBM_NODE_COORDS
+  if (x >= g.lx || y >= g.ly) return;
+  rho_int[node_index(g, x, y, z)] = rho_ref[ref_index(g, x, y, z)];
+}
+
+// field: 0 rho, 1 pressure, 2 psi, 5 fluid (as 0/1) -> reference layout.
+template <typename R, typename O>
+__global__ void k_scalar_to_ref(const R* __restrict__ rho,
+                                const uint32_t* __restrict__ mask,
+                                O* __restrict__ out, Geom g, Phys p,
+                                int field) {
+  MLBM_NODE_COORDS
+  if (x >= g.lx || y >= g.ly) return;
+  const R r = rho[node_index(g, x, y, z)];
+  R v;
+  if (field == 0) v = r;
+  else if (field == 1) v = pressure_of<R>(p, r);
+  else if (field == 2) v = psi_of<R>(p, r);
+  else v = R(fluid_at(mask, g, x, y, z) ? 1 : 0);
+  out[ref_index(g, x, y, z)] = (O)v;
+}
+
+__global__ void k_fluid_to_ref(const uint32_t* __restrict__ mask,
+                               uint8_t* __restrict__ out, Geom g) {
+  MLBM_NODE_COORDS
+  if (x >= g.lx || y >= g.ly) return;
+  out[ref_index(g, x, y, z)] = fluid_at(mask, g, x, y, z) ? 1 : 0;
+}
+
+template <typename O>
+__global__ void k_vel_to_ref(const float* __restrict__ vel,
+                             O* __restrict__ out, Geom g) {
+  MLBM_NODE_COORDS
+  if (x >= g.lx || y >= g.ly) return;
+  const long long n = node_index(g, x, y, z), r = ref_index(g, x, y, z);
+  for (int c = 0; c < 3; ++c) out[3 * r + c] = (O)vel[3 * n + c];
+}
+
+// Post-collision populations f*_i in the reference layout [x][y][z][19].
+// Phase 0: f*_i(x) = pop[opp(i)][x].  Phase 1 (fluid nodes): pop[i][x+e_i]
+// when x+e_i is fluid, else pop[opp(i)][x].  Solid nodes keep their
+// initial values, stored at pop[opp(i)][x] in either phase.
+template <typename T, typename O>
+__global__ void k_pop_to_ref(const T* __restrict__ pop,
+                             const uint32_t* __restrict__ mask,
+                             O* __restrict__ out, Geom g, Phys p, int phase) {
+  using R = typename Pop<T>::Real;
+  MLBM_NODE_COORDS
+  if (x >= g.lx || y >= g.ly) return;
+  const long long n = node_index(g, x, y, z), r = ref_index(g, x, y, z);
+  const bool fl = fluid_at(mask, g, x, y, z);
+  const R shift = R(p.rho_shift);
+#pragma unroll
+  for (int i = 0; i < Q; ++i) {
+    const R s = shift * weight<R>(i);
+    long long src = opp(i) * g.plane + n;
+    if (phase == 1 && fl && i != 0) {
+      const int xd = wrapc(x + ex(i), g.lx), yd = wrapc(y + ey(i), g.ly),
+                zd = wrapc(z + ez(i), g.lz);
+      if (fluid_at(mask, g, xd, yd, zd))
+        src = i * g.plane + node_index(g, xd, yd, zd);
+    }
+    out[(long long)Q * r + i] = (O)Pop<T>::ld(pop + src, s);
+  }
+}
+
+// ---- phase statistics ----------------------------------------------------------
+// Per node of the fluid: counts (fluid, liquid, vapour, liquid-solid and
+// liquid-vapour boundary nodes), FP64 sums (mass, liquid/vapour pressure and
+// density) and min/max of rho and p.  calc_cluster, src/multiphase_lbm.cu:
+// 240-316; write_stats, :1061-1072.
+enum { ST_NF, ST_NL, ST_NV, ST_NLS, ST_NLV, ST_MASS, ST_PL, ST_PV, ST_RL,
+       ST_RV, ST_MINR, ST_MAXR, ST_MINP, ST_MAXP, ST_COUNT };
+
+constexpr int kStatThreads = 256;
+
+template <typename R>
+__global__ void __launch_bounds__(kStatThreads)
+    k_stats_partial(const R* __restrict__ rho,
+                    const uint32_t* __restrict__ mask, Geom g, Phys p,
+                    double* __restrict__ partial) {
+  double acc[ST_COUNT];
+#pragma unroll
+  for (int k = 0; k < ST_COUNT; ++k) acc[k] = 0.0;
+  acc[ST_MINR] = 1e9;
+  acc[ST_MAXR] = -1e-9;
+  acc[ST_MINP] = 1e9;
+  acc[ST_MAXP] = -1e-9;
+  const long long total = (long long)g.lx * g.ly * g.lz;
+  const R rhol = R(p.rhol_spinodal), rhog = R(p.rhog_spinodal);
+  for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+       k < total; k += (long long)gridDim.x * blockDim.x) {
+    const int x = (int)(k % g.lx);
+    const long long yz = k / g.lx;
+    const int y = (int)(yz % g.ly), z = (int)(yz / g.ly);
+    if (!fluid_at(mask, g, x, y, z)) continue;
+    const R r = rho[node_index(g, x, y, z)];
+    const R pr = pressure_of<R>(p, r);
+    acc[ST_NF] += 1.0;
+    acc[ST_MASS] += (double)r;
+    if (r > rhol) {
+      acc[ST_NL] += 1.0;
+      acc[ST_PL] += (double)pr;
+      acc[ST_RL] += (double)r;
+      // first neighbour (i = 1..18) that is solid or non-liquid decides
+      for (int i = 1; i < Q; ++i) {
+        const int xn = wrapc(x - ex(i), g.lx), yn = wrapc(y - ey(i), g.ly),
+                  zn = wrapc(z - ez(i), g.lz);
+        if (!fluid_at(mask, g, xn, yn, zn)) { acc[ST_NLS] += 1.0; break; }
+        if (rho[node_index(g, xn, yn, zn)] < rhol) { acc[ST_NLV] += 1.0; break; }
+      }
+    } else if (r < rhog) {
+      acc[ST_NV] += 1.0;
+      acc[ST_PV] += (double)pr;
+      acc[ST_RV] += (double)r;
+    }
+    acc[ST_MINR] = fmin(acc[ST_MINR], (double)r);
+    acc[ST_MAXR] = fmax(acc[ST_MAXR], (double)r);
+    acc[ST_MINP] = fmin(acc[ST_MINP], (double)pr);
+    acc[ST_MAXP] = fmax(acc[ST_MAXP], (double)pr);
+  }
+  // warp then block reduction in a fixed order (deterministic)
+#pragma unroll
+  for (int k = 0; k < ST_COUNT; ++k) {
+    double v = acc[k];
+    for (int off = 16; off > 0; off >>= 1) {
+      const double o = __shfl_down_sync(0xffffffffu, v, off);
+      v = (k == ST_MINR || k == ST_MINP) ? fmin(v, o)
+          : (k == ST_MAXR || k == ST_MAXP) ? fmax(v, o)
+                                            : v + o;
+    }
+    acc[k] = v;
+  }
+  __shared__ double sh[kStatThreads / 32][ST_COUNT];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (lane == 0)
+    for (int k = 0; k < ST_COUNT; ++k) sh[warp][k] = acc[k];
+  __syncthreads();
+  if (threadIdx.x < ST_COUNT) {
+    const int k = threadIdx.x;
+    double v = sh[0][k];
+    for (int w = 1; w < kStatThreads / 32; ++w) {
+      const double o = sh[w][k];
+      v = (k == ST_MINR || k == ST_MINP) ? fmin(v, o)
+          : (k == ST_MAXR || k == ST_MAXP) ? fmax(v, o)
+                                            : v + o;
+    }
+    partial[(long long)blockIdx.x * ST_COUNT + k] = v;
+  }
+}
+
+__global__ void k_stats_final(const double* __restrict__ partial, int nblocks,
+                              double* __restrict__ out) {
+  const int k = threadIdx.x;
+  if (k >= ST_COUNT) return;
+  double v = partial[k];
+  for (int b = 1; b < nblocks; ++b) {
+    const double o = partial[(long long)b * ST_COUNT + k];
+    v = (k == ST_MINR || k == ST_MINP) ? fmin(v, o)
+        : (k == ST_MAXR || k == ST_MAXP) ? fmax(v, o)
+                                          : v + o;
+  }
+  out[k] = v;
+}
+
+// Per-x-plane fluid / liquid node counts (integer atomics: deterministic).
+template <typename R>
+__global__ void k_plane_profile(const R* __restrict__ rho,
+                                const uint32_t* __restrict__ mask, Geom g,
+                                Phys p, unsigned long long* __restrict__ nf,
+                                unsigned long long* __restrict__ nl) {
+  MLBM_NODE_COORDS
+  if (x >= g.lx || y >= g.ly) return;
+  if (!fluid_at(mask, g, x, y, z)) return;
+  atomicAdd(nf + x, 1ull);
+  if (rho[node_index(g, x, y, z)] > R(p.rhol_spinodal)) atomicAdd(nl + x, 1ull);
+}
+
+}  // namespace mlbm

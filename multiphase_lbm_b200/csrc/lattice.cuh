@@ -1,0 +1,183 @@
+// lattice.cuh -- D3Q19 model, storage formats and Shan-Chen physics shared by
+// every kernel of the B200 implementation.
+//
+// Direction order, weights and velocities are the reference's
+// (include/lbm_model.cuh:35-54) so that populations are interchangeable with
+// the reference's collision_f / stream_f arrays.  opposite(i) is i+9 / i-9
+// (include/lbm_model.cuh:24), with opposite(0) = 0.
+#pragma once
+
+#include <cuda_fp16.h>
+#include <stdint.h>
+
+namespace mlbm {
+
+constexpr int Q = 19;
+
+__host__ __device__ constexpr int ex(int i) {
+  return (i == 0 || i == 2 || i == 3 || i == 8 || i == 9 || i == 11 ||
+          i == 12 || i == 17 || i == 18)
+             ? 0
+             : (i < 10 ? -1 : 1);
+}
+__host__ __device__ constexpr int ey(int i) {
+  return (i == 2 || i == 4 || i == 8 || i == 9 || i == 14) ? -1
+         : (i == 5 || i == 11 || i == 13 || i == 17 || i == 18) ? 1
+                                                                : 0;
+}
+__host__ __device__ constexpr int ez(int i) {
+  return (i == 3 || i == 6 || i == 8 || i == 16 || i == 18) ? -1
+         : (i == 7 || i == 9 || i == 12 || i == 15 || i == 17) ? 1
+                                                                : 0;
+}
+__host__ __device__ constexpr int opp(int i) {
+  return i == 0 ? 0 : (i > 9 ? i - 9 : i + 9);
+}
+// Lattice weights t_i (= the Shan-Chen weights w_i, include/lbm_model.cuh:45)
+template <typename R>
+__host__ __device__ constexpr R weight(int i) {
+  return i == 0 ? R(1.0 / 3.0)
+                : ((i <= 3 || (i >= 10 && i <= 12)) ? R(1.0 / 18.0)
+                                                    : R(1.0 / 36.0));
+}
+
+// ---- geometry of one lattice in HBM --------------------------------------
+// Structure of arrays: population i of node (x,y,z) lives at
+//   pop[i * plane + (z * ly + y) * px + x]
+// with the row pitch px a multiple of 32 nodes (128 B in FP32) so that every
+// warp-wide row access is sector aligned.  Scalars (rho) use the same node
+// index.  The solid mask is one bit per node: word (z*ly + y)*wpr + x/32,
+// bit x%32, 1 = fluid.
+struct Geom {
+  int lx, ly, lz;
+  int px;        // row pitch in nodes (multiple of 32)
+  int wpr;       // mask words per row = px / 32
+  long long plane;  // nodes per population plane = lz * ly * px
+};
+
+__device__ __forceinline__ long long node_index(const Geom& g, int x, int y,
+                                                int z) {
+  return ((long long)z * g.ly + y) * g.px + x;
+}
+__device__ __forceinline__ int wrapc(int v, int n) {
+  return v < 0 ? v + n : (v >= n ? v - n : v);
+}
+__device__ __forceinline__ bool fluid_at(const uint32_t* __restrict__ mask,
+                                         const Geom& g, int x, int y, int z) {
+  uint32_t w = __ldg(mask + ((long long)z * g.ly + y) * g.wpr + (x >> 5));
+  return (w >> (x & 31)) & 1u;
+}
+
+// ---- population storage formats --------------------------------------------
+// FP32 and FP64 store f_i as is.  FP16 stores h_i = half(f_i - t_i * rho0)
+// (shift by the lattice weight times a reference density); arithmetic stays
+// in FP32.
+template <typename T>
+struct Pop;
+
+template <>
+struct Pop<float> {
+  using Real = float;
+  static __device__ __forceinline__ float ld(const float* p, float) {
+    return *p;
+  }
+  static __device__ __forceinline__ void st(float* p, float v, float) {
+    *p = v;
+  }
+};
+template <>
+struct Pop<double> {
+  using Real = double;
+  static __device__ __forceinline__ double ld(const double* p, double) {
+    return *p;
+  }
+  static __device__ __forceinline__ void st(double* p, double v, double) {
+    *p = v;
+  }
+};
+template <>
+struct Pop<__half> {
+  using Real = float;
+  static __device__ __forceinline__ float ld(const __half* p, float shift) {
+    return __half2float(*p) + shift;
+  }
+  static __device__ __forceinline__ void st(__half* p, float v, float shift) {
+    *p = __float2half_rn(v - shift);
+  }
+};
+
+// ---- physics parameters ----------------------------------------------------
+struct Phys {
+  float tau, G, T_Tc, rhol_spinodal, rhog_spinodal, rhos;
+  float rho_increment, inject_position;
+  int carn_star;
+  unsigned long long rho_inject_period;  // 0: never inject
+  int inlet_width, outlet_width;
+  float rho_inlet, rho_outlet;
+  float rho_shift;  // FP16 storage shift (rho0)
+};
+
+// Per-launch step arguments of the reference's multiphaselbm_iteration
+// (include/iteration_host.h:56-57).
+struct StepArgs {
+  long long step;
+  int reverse;
+  unsigned inject_type;
+};
+
+__device__ __forceinline__ float expr(float v) { return expf(v); }
+__device__ __forceinline__ double expr(double v) { return exp(v); }
+
+// dPress, include/iteration_device.cuh:7-27
+template <typename R>
+__device__ __forceinline__ R pressure_of(const Phys& p, R rho) {
+  if (p.carn_star) {
+    const R a = R(1.0), b = R(4.0), Rg = R(1.0), Tc = R(0.0943);
+    R T = R(p.T_Tc) * Tc;
+    R eta = b * rho / R(4.0);
+    R eta2 = eta * eta, eta3 = eta2 * eta, rho2 = rho * rho;
+    R ome = R(1.0) - eta;
+    R ome3 = ome * ome * ome;
+    return rho * Rg * T * (R(1) + eta + eta2 - eta3) / ome3 - a * rho2;
+  }
+  const R cs2 = R(1.0 / 3.0);
+  R psi = R(1.0) - expr(-rho);
+  return cs2 * rho + cs2 * R(p.G) / R(2) * (psi * psi);
+}
+
+// dPsi, include/iteration_device.cuh:31-38
+template <typename R>
+__device__ __forceinline__ R psi_of(const Phys& p, R rho) {
+  if (p.carn_star) {
+    const R cs2 = R(1.0 / 3.0);
+    R pr = pressure_of<R>(p, rho);
+    return sqrt(R(2.0) * (pr - cs2 * rho) / (cs2 * R(p.G)));
+  }
+  return R(1.0) - expr(-rho);
+}
+
+// 0: interior fluid node, 1: inlet slab, 2: outlet slab (drainage boundary,
+// held at fixed density; absent from the reference, defined by this build).
+__device__ __forceinline__ int bc_kind(const Phys& p, const Geom& g, int x) {
+  return x < p.inlet_width ? 1 : (x >= g.lx - p.outlet_width ? 2 : 0);
+}
+
+// Density injection of compute_density, include/iteration_device.cuh:46-59.
+template <typename R>
+__device__ __forceinline__ R inject(const Phys& p, const Geom& g,
+                                    const StepArgs& s, int y, R d) {
+  if (p.rho_inject_period != 0 &&
+      (float)y < p.inject_position * (float)g.ly &&
+      (unsigned long long)s.step % p.rho_inject_period == 0ull) {
+    const R inc = R(p.rho_increment) * R(s.reverse);
+    switch (s.inject_type) {
+      case 0: d += inc; break;
+      case 1: if (d < R(p.rhol_spinodal)) d += inc; break;
+      case 2: if (d > R(p.rhol_spinodal)) d += inc; break;
+      default: break;
+    }
+  }
+  return d;
+}
+
+}  // namespace mlbm
