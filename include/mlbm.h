@@ -188,6 +188,28 @@ mlbm_status mlbm_phase_stats(mlbm_lattice* lat, mlbm_stats* out);
 mlbm_status mlbm_plane_profile(mlbm_lattice* lat, int64_t* n_fluid_x,
                                int64_t* n_liquid_x);
 
+/* Phase statistics without any allocation.  No counterpart in the
+ * reference: it exists for callers that cannot call cudaMalloc when they need
+ * statistics (inside a CUDA graph capture sequence, under a device-memory
+ * budget owned by their own allocator, or embedded in an application that
+ * forbids library allocations).  Same results as mlbm_phase_stats, computed
+ * from fields the caller owns: rho_dev (float) and is_fluid_dev (uint8,
+ * nonzero = fluid), both device arrays in the reference layout [x][y][z]
+ * (z fastest); the EOS and thresholds come from *params.  Runs on `stream`
+ * (NULL = legacy default) and waits for it; *out is host memory.
+ * Its scratch is a fixed static device array (about 459 KB on every GPU that
+ * loads the library, kept until exit), so lx may not exceed
+ * MLBM_NOALLOC_MAX_LX (MLBM_ERR_ARG otherwise).  The first call on each
+ * device looks up the array's device address; make it before any stream
+ * capture starts.  Calls share the array: calls that overlap on the GPU race
+ * and must be serialised by the caller. */
+#define MLBM_NOALLOC_MAX_LX 4096
+mlbm_status mlbm_phase_stats_noalloc(const float* rho_dev,
+                                     const uint8_t* is_fluid_dev, int32_t lx,
+                                     int32_t ly, int32_t lz,
+                                     const mlbm_params* params, void* stream,
+                                     mlbm_stats* out);
+
 /* Information about the lattice: dims[3], storage, phase of the stored
  * state (0/1, see kernels), initialised flag. */
 mlbm_status mlbm_lattice_info(const mlbm_lattice* lat, int32_t* dims,
