@@ -197,7 +197,7 @@ def run_reference_arm(args, rank, world):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--steps", type=int, default=2000)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--storage", default="f32", choices=["f32", "f16", "f64"])
@@ -296,7 +296,7 @@ def main():
                      "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 4),
                      "traffic": traffic, "peak_kind": peak_kind,
-                     "kernel": "time step (density + update kernels)",
+                     "kernel": "time step (k_density + k_update)",
                      "alg_bytes_per_step": int(alg_bytes)},
         "clocks": clocks.summary(),
         "gpu_launches": 2 * args.steps,

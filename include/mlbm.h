@@ -172,6 +172,23 @@ mlbm_status mlbm_iterate(mlbm_lattice* lat, int64_t step0, int32_t nsteps,
                          int32_t reverse, uint32_t inject_type,
                          uint32_t flags);
 
+/* Which kernels advance the lattice: the two-pass kernels (a density launch
+ * and an update launch per step; AUTO, the default) or the fused persistent
+ * kernel (one cooperative launch per step, density and update passes
+ * interleaved plane by plane).  Both give bit-identical results. */
+#define MLBM_KERNEL_AUTO 0
+#define MLBM_KERNEL_FUSED 1
+#define MLBM_KERNEL_TWO_PASS 2
+mlbm_status mlbm_set_step_kernel(mlbm_lattice* lat, int32_t kind);
+/* Tuning of the fused kernel: rows per work item (0 = automatic) and the
+ * plane lag between a plane's density pass and its update pass (0 = 4). */
+mlbm_status mlbm_set_tuning(mlbm_lattice* lat, int32_t rows_per_item,
+                            int32_t plane_lag);
+/* Wait for the lattice's stream and report a device-side failure (a bounded
+ * wait of the fused kernel that ran out: MLBM_ERR_TIMEOUT; the lattice must
+ * then be initialised again). */
+mlbm_status mlbm_synchronize(mlbm_lattice* lat);
+
 /* Copy a field out in the reference layout.  dtype: MLBM_DTYPE_F32 or
  * MLBM_DTYPE_F64 (F64 keeps an FP64 lattice's full precision), U8 for
  * MLBM_FIELD_FLUID.  host_out: lx*ly*lz*components elements.  Synchronous. */

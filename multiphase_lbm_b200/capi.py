@@ -20,6 +20,7 @@ FIELD_RHO, FIELD_PRESSURE, FIELD_PSI, FIELD_VELOCITY, FIELD_POPULATIONS, \
     FIELD_FLUID = range(6)
 DTYPE_F32, DTYPE_F64, DTYPE_U8 = 0, 1, 2
 ITER_WRITE_VELOCITY = 1
+KERNEL_AUTO, KERNEL_FUSED, KERNEL_TWO_PASS = 0, 1, 2
 Q = 19
 
 STATUS = {0: "MLBM_OK", 1: "MLBM_ERR_ARG", 2: "MLBM_ERR_CUDA",
@@ -107,6 +108,12 @@ SIGNATURES = [
     ("mlbm_phase_stats", C.c_int, [_VP, C.POINTER(Stats)]),
     ("mlbm_plane_profile", C.c_int, [_VP, _VP, _VP]),
     ("mlbm_lattice_info", C.c_int, [_VP, _VP, _VP, _VP, _VP]),
+    ("mlbm_set_step_kernel", C.c_int, [_VP, C.c_int32]),
+    ("mlbm_set_tuning", C.c_int, [_VP, C.c_int32, C.c_int32]),
+    ("mlbm_synchronize", C.c_int, [_VP]),
+    ("mlbm_phase_stats_noalloc", C.c_int, [_VP, _VP, C.c_int32, C.c_int32,
+                                           C.c_int32, C.POINTER(Params), _VP,
+                                           C.POINTER(Stats)]),
 ]
 
 
@@ -168,6 +175,15 @@ class Lattice:
 
     def set_stream(self, stream_ptr: int) -> None:
         check(lib().mlbm_set_stream(self.h, C.c_void_p(stream_ptr)))
+
+    def set_step_kernel(self, kind: int) -> None:
+        check(lib().mlbm_set_step_kernel(self.h, kind))
+
+    def set_tuning(self, rows_per_item: int = 0, plane_lag: int = 0) -> None:
+        check(lib().mlbm_set_tuning(self.h, rows_per_item, plane_lag))
+
+    def synchronize(self) -> None:
+        check(lib().mlbm_synchronize(self.h))
 
     def set_params(self, params: Params) -> None:
         check(lib().mlbm_set_params(self.h, C.byref(params)))

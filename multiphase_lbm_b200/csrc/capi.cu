@@ -16,6 +16,7 @@
 #include "capi_internal.h"
 #include "io_kernels.cuh"
 #include "kernels.cuh"
+#include "persistent.cuh"
 
 using namespace mlbm;
 
@@ -110,46 +111,67 @@ mlbm_status activate(const mlbm_lattice* lat) {
 }
 
 template <typename T>
-mlbm_status launch_steps(mlbm_lattice* lat, int64_t step0, int32_t nsteps,
-                         int32_t reverse, uint32_t inject_type,
-                         uint32_t flags) {
+mlbm_status launch_two_pass(mlbm_lattice* lat, const StepArgs& a, bool wu) {
   using R = typename Pop<T>::Real;
   T* pop = static_cast<T*>(lat->pop);
   R* rho = static_cast<R*>(lat->rho);
   R* psi = static_cast<R*>(lat->psi);
   const dim3 grid = node_grid(lat->g), block = node_block();
+  if (lat->phase == 0) {
+    k_density<T, 0><<<grid, block, 0, lat->stream>>>(pop, lat->nbw, rho, psi,
+                                                     lat->g, lat->phys, a);
+    if (wu)
+      k_update<T, 0, true><<<grid, block, 0, lat->stream>>>(
+          pop, lat->nbw, rho, psi, lat->vel, lat->g, lat->phys, a);
+    else
+      k_update<T, 0, false><<<grid, block, 0, lat->stream>>>(
+          pop, lat->nbw, rho, psi, lat->vel, lat->g, lat->phys, a);
+  } else {
+    k_density<T, 1><<<grid, block, 0, lat->stream>>>(pop, lat->nbw, rho, psi,
+                                                     lat->g, lat->phys, a);
+    if (wu)
+      k_update<T, 1, true><<<grid, block, 0, lat->stream>>>(
+          pop, lat->nbw, rho, psi, lat->vel, lat->g, lat->phys, a);
+    else
+      k_update<T, 1, false><<<grid, block, 0, lat->stream>>>(
+          pop, lat->nbw, rho, psi, lat->vel, lat->g, lat->phys, a);
+  }
+  CUDA_TRY(cudaGetLastError(), "time-step launch");
+  return MLBM_OK;
+}
+
+// One lattice step per launch (two launches for the two-pass kernels, which
+// AUTO selects).  The fused persistent kernel writes rho only when asked (the
+// last step of each mlbm_iterate call); the two-pass kernels write it every
+// step.
+template <typename T>
+mlbm_status launch_steps(mlbm_lattice* lat, int64_t step0, int32_t nsteps,
+                         int32_t reverse, uint32_t inject_type,
+                         uint32_t flags) {
+  const bool fused = lat->step_kernel == MLBM_KERNEL_FUSED && lat->fused.ok;
+  if (lat->step_kernel == MLBM_KERNEL_FUSED && !lat->fused.ok)
+    return fail(MLBM_ERR_ARG, "fused kernel does not fit this lattice");
   for (int32_t s = 0; s < nsteps; ++s) {
     StepArgs a{(long long)(step0 + s), reverse, inject_type};
-    const bool wu = (flags & MLBM_ITER_WRITE_VELOCITY) && s == nsteps - 1;
-    if (lat->phase == 0) {
-      k_density<T, 0><<<grid, block, 0, lat->stream>>>(pop, lat->mask, rho, psi,
-                                                       lat->g, lat->phys, a);
-      if (wu)
-        k_update<T, 0, true><<<grid, block, 0, lat->stream>>>(
-            pop, lat->mask, rho, psi, lat->vel, lat->g, lat->phys, a);
-      else
-        k_update<T, 0, false><<<grid, block, 0, lat->stream>>>(
-            pop, lat->mask, rho, psi, lat->vel, lat->g, lat->phys, a);
-    } else {
-      k_density<T, 1><<<grid, block, 0, lat->stream>>>(pop, lat->mask, rho, psi,
-                                                       lat->g, lat->phys, a);
-      if (wu)
-        k_update<T, 1, true><<<grid, block, 0, lat->stream>>>(
-            pop, lat->mask, rho, psi, lat->vel, lat->g, lat->phys, a);
-      else
-        k_update<T, 1, false><<<grid, block, 0, lat->stream>>>(
-            pop, lat->mask, rho, psi, lat->vel, lat->g, lat->phys, a);
-    }
+    const bool last = s == nsteps - 1;
+    const bool wu = (flags & MLBM_ITER_WRITE_VELOCITY) && last;
+    mlbm_status st;
+    if (fused)
+      st = launch_fused<T>(lat, a, wu ? (OUT_RHO | OUT_VEL) : (last ? OUT_RHO : OUT_NONE));
+    else
+      st = launch_two_pass<T>(lat, a, wu);
+    if (st) return st;
     lat->phase ^= 1;
     if (wu) lat->vel_valid = true;
   }
-  CUDA_TRY(cudaGetLastError(), "time-step launch");
   return MLBM_OK;
 }
 
 template <typename T>
 mlbm_status launch_init(mlbm_lattice* lat) {
   using R = typename Pop<T>::Real;
+  k_build_nbr<<<node_grid(lat->g), node_block(), 0, lat->stream>>>(
+      lat->mask, lat->nbw, lat->g, lat->phys);
   k_init<T><<<node_grid(lat->g), node_block(), 0, lat->stream>>>(
       static_cast<T*>(lat->pop), lat->mask, lat->rho_init,
       static_cast<R*>(lat->rho), static_cast<R*>(lat->psi), lat->g, lat->phys);
@@ -211,6 +233,22 @@ size_t field_components(int32_t field) {
                                            : 1;
 }
 
+// After a stream synchronisation: report (and clear) a wait timeout raised by
+// the fused kernel.  The interrupted step left the lattice inconsistent.
+mlbm_status check_device_error(mlbm_lattice* lat) {
+  int h = 0;
+  CUDA_TRY(cudaMemcpy(&h, lat->err, sizeof(int), cudaMemcpyDeviceToHost),
+           "error flag read");
+  if (!h) return MLBM_OK;
+  cudaMemset(lat->err, 0, sizeof(int));
+  cudaMemset(lat->pdone, 0, sizeof(unsigned) * lat->g.lz);
+  lat->fused_epoch = 0;
+  lat->initialized = false;
+  return fail(MLBM_ERR_TIMEOUT,
+              "a bounded wait of the fused time step ran out; the lattice "
+              "must be initialised again");
+}
+
 mlbm_status ensure_staging(mlbm_lattice* lat, size_t bytes) {
   if (lat->staging_bytes >= bytes) return MLBM_OK;
   if (lat->staging) cudaFree(lat->staging);
@@ -264,7 +302,8 @@ uint64_t mlbm_lattice_bytes(int32_t lx, int32_t ly, int32_t lz,
          + 2 * np * real_bytes(storage)       // rho, psi
          + np * 4                             // initial density
          + (uint64_t)g.lz * g.ly * g.wpr * 4  // mask
-         + np * 12;                           // velocity
+         + np * 12                            // velocity
+         + np * 4;                            // neighbour words
 }
 
 mlbm_status mlbm_lattice_create(int32_t lx, int32_t ly, int32_t lz,
@@ -275,6 +314,8 @@ mlbm_status mlbm_lattice_create(int32_t lx, int32_t ly, int32_t lz,
   if (lx < 1 || ly < 1 || lz < 1 || lz > 65535 || ly > (1 << 24) ||
       lx > (1 << 24))
     return fail(MLBM_ERR_ARG, "invalid lattice size %d x %d x %d", lx, ly, lz);
+  if (make_geom(lx, ly, lz).plane >= (1LL << 31))
+    return fail(MLBM_ERR_ARG, "lattice too large (more than 2^31 padded nodes)");
   if (storage < MLBM_STORE_F32 || storage > MLBM_STORE_F64)
     return fail(MLBM_ERR_ARG, "invalid storage %d", storage);
   int ndev = 0;
@@ -288,6 +329,7 @@ mlbm_status mlbm_lattice_create(int32_t lx, int32_t ly, int32_t lz,
   lat->device = device;
   lat->storage = storage;
   lat->g = make_geom(lx, ly, lz);
+  lat->fused = fused_shape(lat->g, storage, 0, 0);
   const size_t np = (size_t)lat->g.plane;
   const size_t mask_words = (size_t)lz * ly * lat->g.wpr;
   cudaError_t e = cudaSuccess;
@@ -300,6 +342,11 @@ mlbm_status mlbm_lattice_create(int32_t lx, int32_t ly, int32_t lz,
   alloc((void**)&lat->rho_init, np * sizeof(float));
   alloc((void**)&lat->mask, mask_words * sizeof(uint32_t));
   alloc((void**)&lat->vel, np * 3 * sizeof(float));
+  alloc((void**)&lat->nbw, np * sizeof(uint32_t));
+  alloc((void**)&lat->pdone, (size_t)lz * sizeof(unsigned));
+  alloc((void**)&lat->err, sizeof(int));
+  if (e == cudaSuccess) e = cudaMemset(lat->pdone, 0, (size_t)lz * sizeof(unsigned));
+  if (e == cudaSuccess) e = cudaMemset(lat->err, 0, sizeof(int));
   if (e == cudaSuccess) e = cudaMemset(lat->mask, 0, mask_words * 4);
   if (e == cudaSuccess) e = cudaMemset(lat->rho_init, 0, np * sizeof(float));
   if (e != cudaSuccess) {
@@ -321,8 +368,11 @@ mlbm_status mlbm_lattice_destroy(mlbm_lattice* lat) {
   cudaFree(lat->rho_init);
   cudaFree(lat->mask);
   cudaFree(lat->vel);
+  cudaFree(lat->nbw);
   cudaFree(lat->staging);
   cudaFree(lat->stats_scratch);
+  cudaFree(lat->pdone);
+  cudaFree(lat->err);
   delete lat;
   return MLBM_OK;
 }
@@ -482,7 +532,7 @@ mlbm_status mlbm_download_field(mlbm_lattice* lat, int32_t field,
                            cudaMemcpyDeviceToHost, lat->stream),
            "field download copy");
   CUDA_TRY(cudaStreamSynchronize(lat->stream), "field download");
-  return MLBM_OK;
+  return check_device_error(lat);
 }
 
 mlbm_status mlbm_phase_stats(mlbm_lattice* lat, mlbm_stats* out) {
@@ -520,6 +570,7 @@ mlbm_status mlbm_phase_stats(mlbm_lattice* lat, mlbm_stats* out) {
   CUDA_TRY(cudaMemcpyAsync(h, fin, sizeof h, cudaMemcpyDeviceToHost, lat->stream),
            "stats copy");
   CUDA_TRY(cudaStreamSynchronize(lat->stream), "stats");
+  if (mlbm_status st = check_device_error(lat)) return st;
   std::memset(out, 0, sizeof *out);
   out->n_fluid = (int64_t)h[ST_NF];
   out->n_liquid = (int64_t)h[ST_NL];
@@ -575,6 +626,40 @@ mlbm_status mlbm_plane_profile(mlbm_lattice* lat, int64_t* n_fluid_x,
                            lat->stream), "profile copy");
   CUDA_TRY(cudaStreamSynchronize(lat->stream), "profile");
   return MLBM_OK;
+}
+
+mlbm_status mlbm_set_step_kernel(mlbm_lattice* lat, int32_t kind) {
+  if (mlbm_status st = check_lat(lat)) return st;
+  if (kind < MLBM_KERNEL_AUTO || kind > MLBM_KERNEL_TWO_PASS)
+    return fail(MLBM_ERR_ARG, "invalid step kernel %d", kind);
+  if (kind == MLBM_KERNEL_FUSED && !lat->fused.ok)
+    return fail(MLBM_ERR_ARG, "fused kernel does not fit this lattice");
+  lat->step_kernel = kind;
+  return MLBM_OK;
+}
+
+mlbm_status mlbm_set_tuning(mlbm_lattice* lat, int32_t rows_per_item,
+                            int32_t plane_lag) {
+  if (mlbm_status st = check_lat(lat)) return st;
+  if (rows_per_item < 0 || plane_lag < 0 || rows_per_item > 512)
+    return fail(MLBM_ERR_ARG, "invalid tuning");
+  const FusedShape f = fused_shape(lat->g, lat->storage, rows_per_item, plane_lag);
+  if (!f.ok) return fail(MLBM_ERR_ARG, "tuning does not fit the fused kernel");
+  if (mlbm_status st = activate(lat)) return st;
+  // the per-plane counters count items, so a new item size restarts them
+  CUDA_TRY(cudaStreamSynchronize(lat->stream), "tuning sync");
+  CUDA_TRY(cudaMemset(lat->pdone, 0, sizeof(unsigned) * lat->g.lz), "counter reset");
+  lat->fused = f;
+  lat->fused_epoch = 0;
+  for (int& v : lat->fused_grid) v = 0;
+  return MLBM_OK;
+}
+
+mlbm_status mlbm_synchronize(mlbm_lattice* lat) {
+  if (mlbm_status st = check_lat(lat)) return st;
+  if (mlbm_status st = activate(lat)) return st;
+  CUDA_TRY(cudaStreamSynchronize(lat->stream), "synchronize");
+  return check_device_error(lat);
 }
 
 mlbm_status mlbm_lattice_info(const mlbm_lattice* lat, int32_t* dims,

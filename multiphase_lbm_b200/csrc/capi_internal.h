@@ -7,6 +7,15 @@
 #include "errors.h"
 #include "lattice.cuh"
 
+namespace mlbm {
+// Launch geometry of the fused persistent time step (persistent.cuh).
+struct FusedShape {
+  int W, nseg, By, threads, rb_y, R, L;
+  size_t smem;
+  bool ok;  // fits (shared memory, threads); otherwise the two-pass kernels
+};
+}  // namespace mlbm
+
 struct mlbm_lattice {
   int device = 0;
   int storage = MLBM_STORE_F32;
@@ -21,11 +30,20 @@ struct mlbm_lattice {
   void* psi = nullptr;          // pseudopotential, R per node
   float* rho_init = nullptr;    // uploaded initial density (internal layout)
   uint32_t* mask = nullptr;     // 1 bit per node, 1 = fluid
+  uint32_t* nbw = nullptr;      // per-node neighbour word (kernels.cuh)
   float* vel = nullptr;         // [node][3], written on request
   void* staging = nullptr;      // reference-layout transfer buffer
   size_t staging_bytes = 0;
   double* stats_scratch = nullptr;
   size_t stats_scratch_bytes = 0;
+
+  // fused persistent step
+  mlbm::FusedShape fused{};
+  int fused_grid[6] = {0, 0, 0, 0, 0, 0};  // per (phase, output) variant
+  unsigned long long fused_epoch = 0;      // launches since counter reset
+  unsigned* pdone = nullptr;               // per-plane completion counters
+  int* err = nullptr;                      // device error flag (wait timeout)
+  int step_kernel = 0;                     // MLBM_KERNEL_*
 
   int phase = 0;  // 0: post-collision at opp slots of own node; 1: pushed
   bool has_params = false, has_mask = false, has_rho = false;
@@ -38,4 +56,8 @@ mlbm_status cuda_fail(cudaError_t e, const char* where);
 size_t pop_elem_bytes(int storage);
 size_t real_bytes(int storage);
 Geom make_geom(int lx, int ly, int lz);
+FusedShape fused_shape(const Geom& g, int storage, int by_hint, int lag);
+struct StepArgs;
+template <typename T>
+mlbm_status launch_fused(mlbm_lattice* lat, const StepArgs& a, int out);
 }  // namespace mlbm

@@ -1,4 +1,5 @@
-// kernels.cuh -- the time-step kernels of the D3Q19 Shan-Chen update.
+// kernels.cuh -- per-node building blocks of the D3Q19 Shan-Chen update and
+// the two-pass time-step kernels.
 //
 // One lattice buffer, updated in place with the AA access pattern.  The
 // stored state alternates between two forms:
@@ -15,83 +16,184 @@
 //
 // Every step is two passes:
 //   density pass  (compute_density, include/iteration_device.cuh:40-63):
-//                 rho = sum_i f_i (+ injection) for every fluid node;
+//                 rho = sum_i f_i (+ injection) for every fluid node, psi(rho);
 //   update pass   (compute_force / compute_velocity / post_collision,
 //                 include/iteration_device.cuh:69-206): Shan-Chen force from
-//                 psi(rho) of the 18 neighbours, velocity shift, BGK, store.
+//                 psi of the 18 neighbours, velocity shift, BGK, store.
 // The update pass recomputes the same rho bit for bit from the same loads.
+//
+// Per-node neighbour word (built once by k_build_nbr): bit 0 = the node is
+// fluid; bit i (1..18) = the pull source x - e_i is fluid; bits 19-20 = the
+// drainage slab kind (0 interior, 1 inlet, 2 outlet).
 #pragma once
 
 #include "lattice.cuh"
 
 namespace mlbm {
 
-// Load the 19 pre-collision populations of node (x,y,z) for a step that
-// starts in `PHASE`.
+constexpr uint32_t NB_SELF = 1u;
+__host__ __device__ constexpr int nb_kind(uint32_t nb) { return (nb >> 19) & 3; }
+
+// Wrapped neighbour offsets of one node: x-1, x, x+1 and the 9 row offsets
+// of (y+dy, z+dz), dy, dz in {-1, 0, 1}.  Node indices fit 32 bits (checked
+// when the lattice is created).
+struct Nbr {
+  int xm, x0, xp;
+  int r[3][3];
+  __device__ __forceinline__ void init(const Geom& g, int x, int y, int z) {
+    xm = x == 0 ? g.lx - 1 : x - 1;
+    x0 = x;
+    xp = x == g.lx - 1 ? 0 : x + 1;
+    const int ys[3] = {y == 0 ? g.ly - 1 : y - 1, y, y == g.ly - 1 ? 0 : y + 1};
+    const int zs[3] = {z == 0 ? g.lz - 1 : z - 1, z, z == g.lz - 1 ? 0 : z + 1};
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+      for (int b = 0; b < 3; ++b) r[a][b] = (zs[b] * g.ly + ys[a]) * g.px;
+  }
+  __device__ __forceinline__ int idx(int dx, int dy, int dz) const {
+    return r[dy + 1][dz + 1] + (dx < 0 ? xm : (dx > 0 ? xp : x0));
+  }
+};
+
+// Gather the 19 pre-collision populations of a fluid node for a step that
+// starts in `PHASE` (see the header comment).
 template <typename T, int PHASE>
-__device__ __forceinline__ void load_pre(
-    const T* __restrict__ pop, const uint32_t* __restrict__ mask,
-    const Geom& g, int x, int y, int z, long long n,
-    typename Pop<T>::Real shift, typename Pop<T>::Real (&f)[Q]) {
+__device__ __forceinline__ void gather(const T* __restrict__ pop,
+                                       long long plane, const Nbr& a,
+                                       uint32_t nb, int n,
+                                       typename Pop<T>::Real shift,
+                                       typename Pop<T>::Real (&f)[Q]) {
   using R = typename Pop<T>::Real;
 #pragma unroll
   for (int i = 0; i < Q; ++i) {
     const R s = shift * weight<R>(i);
-    if (PHASE == 1 || i == 0) {
-      f[i] = Pop<T>::ld(pop + i * g.plane + n, s);
-    } else {
-      const int xs = wrapc(x - ex(i), g.lx), ys = wrapc(y - ey(i), g.ly),
-                zs = wrapc(z - ez(i), g.lz);
-      if (fluid_at(mask, g, xs, ys, zs))
-        f[i] = Pop<T>::ld(pop + opp(i) * g.plane + node_index(g, xs, ys, zs), s);
-      else
-        f[i] = Pop<T>::ld(pop + i * g.plane + n, s);
+    int src = n, slot = i;
+    if (PHASE == 0 && i != 0 && ((nb >> i) & 1u)) {
+      src = a.idx(-ex(i), -ey(i), -ez(i));
+      slot = opp(i);
     }
+    f[i] = Pop<T>::ld(pop + (long long)slot * plane + src, s);
   }
 }
 
-// Store the 19 post-collision populations of node (x,y,z) for a step that
+// Store the 19 post-collision populations of a fluid node for a step that
 // started in `PHASE`.
 template <typename T, int PHASE>
-__device__ __forceinline__ void store_post(
-    T* __restrict__ pop, const uint32_t* __restrict__ mask, const Geom& g,
-    int x, int y, int z, long long n, typename Pop<T>::Real shift,
-    const typename Pop<T>::Real (&f)[Q]) {
+__device__ __forceinline__ void scatter(T* __restrict__ pop, long long plane,
+                                        const Nbr& a, uint32_t nb, int n,
+                                        typename Pop<T>::Real shift,
+                                        const typename Pop<T>::Real (&f)[Q]) {
   using R = typename Pop<T>::Real;
 #pragma unroll
   for (int i = 0; i < Q; ++i) {
     const R s = shift * weight<R>(i);
-    if (PHASE == 1 || i == 0) {
-      Pop<T>::st(pop + opp(i) * g.plane + n, f[i], s);
-    } else {
-      const int xd = wrapc(x + ex(i), g.lx), yd = wrapc(y + ey(i), g.ly),
-                zd = wrapc(z + ez(i), g.lz);
-      if (fluid_at(mask, g, xd, yd, zd))
-        Pop<T>::st(pop + i * g.plane + node_index(g, xd, yd, zd), f[i], s);
-      else
-        Pop<T>::st(pop + opp(i) * g.plane + n, f[i], s);
+    int dst = n, slot = opp(i);
+    // x + e_i is fluid  <=>  the pull source of direction opp(i) is fluid
+    if (PHASE == 0 && i != 0 && ((nb >> opp(i)) & 1u)) {
+      dst = a.idx(ex(i), ey(i), ez(i));
+      slot = i;
     }
+    Pop<T>::st(pop + (long long)slot * plane + dst, f[i], s);
   }
 }
 
-// rho of a fluid node from its pre-collision populations, summed in the
-// reference's order i = 0..18, plus injection; fixed at the drainage slabs.
+// rho of an interior fluid node from its pre-collision populations, summed in
+// the reference's order i = 0..18, plus injection.
 template <typename R>
-__device__ __forceinline__ R node_density(const Phys& p, const Geom& g,
-                                          const StepArgs& s, int x, int y,
-                                          const R (&f)[Q]) {
-  const int bc = bc_kind(p, g, x);
-  if (bc) return R(bc == 1 ? p.rho_inlet : p.rho_outlet);
+__device__ __forceinline__ R sum_density(const Phys& p, const Geom& g,
+                                         const StepArgs& s, int y,
+                                         const R (&f)[Q]) {
   R d = R(0);
 #pragma unroll
-  for (int i = 0; i < Q; ++i) d += f[i];
+  for (int i = 0; i < Q; ++i) d = radd(d, f[i]);
   return inject<R>(p, g, s, y, d);
 }
 
-// ---- density pass ------------------------------------------------------------
+__device__ __forceinline__ float slab_density(const Phys& p, int kind) {
+  return kind == 1 ? p.rho_inlet : p.rho_outlet;
+}
+
+// Force, velocity shift and BGK relaxation of one interior fluid node
+// (include/iteration_device.cuh:69-206).  psi_nb(i) returns psi at x + e_i.
+template <typename R, typename PsiNb>
+__device__ __forceinline__ void collide(const Phys& p, R d, R psi_self,
+                                        PsiNb psi_nb, R (&f)[Q], R& ux, R& uy,
+                                        R& uz) {
+  // F = -G psi(x) sum_{i=1..18} w_i psi(x + e_i) e_i, terms in order i
+  R sx = R(0), sy = R(0), sz = R(0);
+#pragma unroll
+  for (int i = 1; i < Q; ++i) {
+    const R wp = rmul(weight<R>(i), psi_nb(i));
+    if (ex(i)) sx = ex(i) > 0 ? radd(sx, wp) : rsub(sx, wp);
+    if (ey(i)) sy = ey(i) > 0 ? radd(sy, wp) : rsub(sy, wp);
+    if (ez(i)) sz = ez(i) > 0 ? radd(sz, wp) : rsub(sz, wp);
+  }
+  const R gp = rmul(-R(p.G), psi_self);
+  const R Fx = rmul(gp, sx), Fy = rmul(gp, sy), Fz = rmul(gp, sz);
+  // u = (sum_i f_i e_i + tau F) / rho
+  ux = R(0);
+  uy = R(0);
+  uz = R(0);
+#pragma unroll
+  for (int i = 0; i < Q; ++i) {
+    if (ex(i)) ux = ex(i) > 0 ? radd(ux, f[i]) : rsub(ux, f[i]);
+    if (ey(i)) uy = ey(i) > 0 ? radd(uy, f[i]) : rsub(uy, f[i]);
+    if (ez(i)) uz = ez(i) > 0 ? radd(uz, f[i]) : rsub(uz, f[i]);
+  }
+  const R tau = R(p.tau);
+  const R inv_rho = rdiv(R(1), d);
+  ux = rmul(rfma(tau, Fx, ux), inv_rho);
+  uy = rmul(rfma(tau, Fy, uy), inv_rho);
+  uz = rmul(rfma(tau, Fz, uz), inv_rho);
+  const R usq15 =
+      rmul(R(1.5), rfma(uz, uz, rfma(uy, uy, rmul(ux, ux))));
+  const R omega = rdiv(R(1), tau);
+  // BGK, include/iteration_device.cuh:162-174:
+  //   f_i += (t_i rho (1 + 3 eu + 4.5 eu^2 - 1.5 u^2) - f_i) / tau
+#pragma unroll
+  for (int i = 0; i < Q; ++i) {
+    R eu = R(0);
+    if (ex(i)) eu = ex(i) > 0 ? radd(eu, ux) : rsub(eu, ux);
+    if (ey(i)) eu = ey(i) > 0 ? radd(eu, uy) : rsub(eu, uy);
+    if (ez(i)) eu = ez(i) > 0 ? radd(eu, uz) : rsub(eu, uz);
+    const R poly = rsub(rfma(rmul(R(4.5), eu), eu, rfma(R(3), eu, R(1))), usq15);
+    const R feq = rmul(rmul(weight<R>(i), d), poly);
+    f[i] = rfma(rsub(feq, f[i]), omega, f[i]);
+  }
+}
+
+// Rest equilibrium of a drainage-slab node (its post-collision populations).
+template <typename R>
+__device__ __forceinline__ void slab_populations(R d, R (&f)[Q]) {
+#pragma unroll
+  for (int i = 0; i < Q; ++i) f[i] = rmul(weight<R>(i), d);
+}
+
+// ---- neighbour words ---------------------------------------------------------
+static __global__ void k_build_nbr(const uint32_t* __restrict__ mask,
+                            uint32_t* __restrict__ nbw, Geom g, Phys p) {
+  const int x = blockIdx.x * 32 + threadIdx.x;
+  const int y = blockIdx.y * blockDim.y + threadIdx.y;
+  const int z = blockIdx.z;
+  if (x >= g.lx || y >= g.ly) return;
+  uint32_t w = 0;
+  if (fluid_at(mask, g, x, y, z)) {
+    w = NB_SELF;
+    for (int i = 1; i < Q; ++i)
+      if (fluid_at(mask, g, wrapc(x - ex(i), g.lx), wrapc(y - ey(i), g.ly),
+                   wrapc(z - ez(i), g.lz)))
+        w |= 1u << i;
+    w |= (uint32_t)bc_kind(p, g, x) << 19;
+  }
+  nbw[node_index(g, x, y, z)] = w;
+}
+
+// ---- two-pass kernels -----------------------------------------------------------
+// blockDim (32, 4): a warp covers 32 x-consecutive nodes of one row.
 template <typename T, int PHASE>
 __global__ void __launch_bounds__(128)
-    k_density(const T* __restrict__ pop, const uint32_t* __restrict__ mask,
+    k_density(const T* __restrict__ pop, const uint32_t* __restrict__ nbw,
               typename Pop<T>::Real* __restrict__ rho,
               typename Pop<T>::Real* __restrict__ psi, Geom g, Phys p,
               StepArgs s) {
@@ -100,27 +202,26 @@ __global__ void __launch_bounds__(128)
   const int y = blockIdx.y * blockDim.y + threadIdx.y;
   const int z = blockIdx.z;
   if (x >= g.lx || y >= g.ly) return;
-  if (!fluid_at(mask, g, x, y, z)) return;
-  const long long n = node_index(g, x, y, z);
+  const int n = (int)node_index(g, x, y, z);
+  const uint32_t nb = nbw[n];
+  if (!(nb & NB_SELF)) return;
   R d;
-  if (bc_kind(p, g, x)) {
-    R dummy[Q];
-#pragma unroll
-    for (int i = 0; i < Q; ++i) dummy[i] = R(0);
-    d = node_density<R>(p, g, s, x, y, dummy);
+  if (nb_kind(nb)) {
+    d = R(slab_density(p, nb_kind(nb)));
   } else {
+    Nbr a;
+    a.init(g, x, y, z);
     R f[Q];
-    load_pre<T, PHASE>(pop, mask, g, x, y, z, n, R(p.rho_shift), f);
-    d = node_density<R>(p, g, s, x, y, f);
+    gather<T, PHASE>(pop, g.plane, a, nb, n, R(p.rho_shift), f);
+    d = sum_density<R>(p, g, s, y, f);
   }
   rho[n] = d;
   psi[n] = psi_of<R>(p, d);
 }
 
-// ---- update pass -------------------------------------------------------------
 template <typename T, int PHASE, bool WRITE_U>
 __global__ void __launch_bounds__(128)
-    k_update(T* __restrict__ pop, const uint32_t* __restrict__ mask,
+    k_update(T* __restrict__ pop, const uint32_t* __restrict__ nbw,
              const typename Pop<T>::Real* __restrict__ rho,
              const typename Pop<T>::Real* __restrict__ psi,
              float* __restrict__ vel, Geom g, Phys p, StepArgs s) {
@@ -129,76 +230,30 @@ __global__ void __launch_bounds__(128)
   const int y = blockIdx.y * blockDim.y + threadIdx.y;
   const int z = blockIdx.z;
   if (x >= g.lx || y >= g.ly) return;
-  if (!fluid_at(mask, g, x, y, z)) return;
-  const long long n = node_index(g, x, y, z);
+  const int n = (int)node_index(g, x, y, z);
+  const uint32_t nb = nbw[n];
+  if (!(nb & NB_SELF)) return;
   const R shift = R(p.rho_shift);
+  Nbr a;
+  a.init(g, x, y, z);
   R f[Q];
-  const int bc = bc_kind(p, g, x);
-  if (bc) {
-    // Drainage slabs: post-collision populations are the rest equilibrium.
-    const R d = R(bc == 1 ? p.rho_inlet : p.rho_outlet);
-#pragma unroll
-    for (int i = 0; i < Q; ++i) f[i] = weight<R>(i) * d;
-    if (WRITE_U) {
-      vel[3 * n] = 0.f;
-      vel[3 * n + 1] = 0.f;
-      vel[3 * n + 2] = 0.f;
-    }
-    store_post<T, PHASE>(pop, mask, g, x, y, z, n, shift, f);
-    return;
-  }
-  load_pre<T, PHASE>(pop, mask, g, x, y, z, n, shift, f);
-  const R d = rho[n];
-
-  // Shan-Chen force, include/iteration_device.cuh:69-152:
-  //   F = -G psi(x) sum_{i=1..18} w_i psi(x + e_i) e_i
-  R sx = R(0), sy = R(0), sz = R(0);
-#pragma unroll
-  for (int i = 1; i < Q; ++i) {
-    const int xn = wrapc(x + ex(i), g.lx), yn = wrapc(y + ey(i), g.ly),
-              zn = wrapc(z + ez(i), g.lz);
-    const R wp = weight<R>(i) * __ldg(psi + node_index(g, xn, yn, zn));
-    if (ex(i)) sx += ex(i) > 0 ? wp : -wp;
-    if (ey(i)) sy += ey(i) > 0 ? wp : -wp;
-    if (ez(i)) sz += ez(i) > 0 ? wp : -wp;
-  }
-  const R gp = -R(p.G) * psi[n];
-  const R Fx = gp * sx, Fy = gp * sy, Fz = gp * sz;
-
-  // Velocity shift, include/iteration_device.cuh:181-206:
-  //   u = (sum_i f_i e_i + tau F) / rho
   R ux = R(0), uy = R(0), uz = R(0);
-#pragma unroll
-  for (int i = 0; i < Q; ++i) {
-    if (ex(i)) ux += ex(i) > 0 ? f[i] : -f[i];
-    if (ey(i)) uy += ey(i) > 0 ? f[i] : -f[i];
-    if (ez(i)) uz += ez(i) > 0 ? f[i] : -f[i];
+  if (nb_kind(nb)) {
+    slab_populations<R>(R(slab_density(p, nb_kind(nb))), f);
+  } else {
+    gather<T, PHASE>(pop, g.plane, a, nb, n, shift, f);
+    const R d = rho[n];
+    collide<R>(
+        p, d, psi[n],
+        [&](int i) { return __ldg(psi + a.idx(ex(i), ey(i), ez(i))); }, f,
+        ux, uy, uz);
   }
-  const R tau = R(p.tau);
-  const R inv_rho = R(1) / d;
-  ux = (ux + tau * Fx) * inv_rho;
-  uy = (uy + tau * Fy) * inv_rho;
-  uz = (uz + tau * Fz) * inv_rho;
   if (WRITE_U) {
-    vel[3 * n] = (float)ux;
-    vel[3 * n + 1] = (float)uy;
-    vel[3 * n + 2] = (float)uz;
+    vel[3 * (long long)n] = (float)ux;
+    vel[3 * (long long)n + 1] = (float)uy;
+    vel[3 * (long long)n + 2] = (float)uz;
   }
-  const R usq15 = R(1.5) * (ux * ux + uy * uy + uz * uz);
-  const R omega = R(1) / tau;
-
-  // BGK relaxation, include/iteration_device.cuh:162-174
-#pragma unroll
-  for (int i = 0; i < Q; ++i) {
-    R eu = R(0);
-    if (ex(i)) eu += ex(i) > 0 ? ux : -ux;
-    if (ey(i)) eu += ey(i) > 0 ? uy : -uy;
-    if (ez(i)) eu += ez(i) > 0 ? uz : -uz;
-    const R feq = weight<R>(i) * d *
-                  (R(1) + R(3) * eu + R(4.5) * eu * eu - usq15);
-    f[i] = f[i] + (feq - f[i]) * omega;
-  }
-  store_post<T, PHASE>(pop, mask, g, x, y, z, n, shift, f);
+  scatter<T, PHASE>(pop, g.plane, a, nb, n, shift, f);
 }
 
 // ---- initialisation (multiphaselbm_init, include/iteration_kernel.cuh:9-29) --

@@ -125,6 +125,19 @@ struct StepArgs {
   unsigned inject_type;
 };
 
+// Rounded arithmetic that the compiler may not contract or reorder, so every
+// kernel that inlines collide() produces the same bits.
+__device__ __forceinline__ float rmul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float radd(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float rsub(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ float rfma(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+__device__ __forceinline__ float rdiv(float a, float b) { return __fdiv_rn(a, b); }
+__device__ __forceinline__ double rmul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double radd(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double rsub(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ double rfma(double a, double b, double c) { return __fma_rn(a, b, c); }
+__device__ __forceinline__ double rdiv(double a, double b) { return __ddiv_rn(a, b); }
+
 __device__ __forceinline__ float expr(float v) { return expf(v); }
 __device__ __forceinline__ double expr(double v) { return exp(v); }
 
@@ -133,16 +146,17 @@ template <typename R>
 __device__ __forceinline__ R pressure_of(const Phys& p, R rho) {
   if (p.carn_star) {
     const R a = R(1.0), b = R(4.0), Rg = R(1.0), Tc = R(0.0943);
-    R T = R(p.T_Tc) * Tc;
-    R eta = b * rho / R(4.0);
-    R eta2 = eta * eta, eta3 = eta2 * eta, rho2 = rho * rho;
-    R ome = R(1.0) - eta;
-    R ome3 = ome * ome * ome;
-    return rho * Rg * T * (R(1) + eta + eta2 - eta3) / ome3 - a * rho2;
+    const R T = rmul(R(p.T_Tc), Tc);
+    const R eta = rdiv(rmul(b, rho), R(4.0));
+    const R eta2 = rmul(eta, eta), eta3 = rmul(eta2, eta), rho2 = rmul(rho, rho);
+    const R ome = rsub(R(1.0), eta);
+    const R ome3 = rmul(rmul(ome, ome), ome);
+    const R num = rsub(radd(radd(R(1), eta), eta2), eta3);
+    return rsub(rdiv(rmul(rmul(rmul(rho, Rg), T), num), ome3), rmul(a, rho2));
   }
   const R cs2 = R(1.0 / 3.0);
-  R psi = R(1.0) - expr(-rho);
-  return cs2 * rho + cs2 * R(p.G) / R(2) * (psi * psi);
+  const R psi = rsub(R(1.0), expr(-rho));
+  return radd(rmul(cs2, rho), rmul(rdiv(rmul(cs2, R(p.G)), R(2)), rmul(psi, psi)));
 }
 
 // dPsi, include/iteration_device.cuh:31-38
@@ -150,10 +164,10 @@ template <typename R>
 __device__ __forceinline__ R psi_of(const Phys& p, R rho) {
   if (p.carn_star) {
     const R cs2 = R(1.0 / 3.0);
-    R pr = pressure_of<R>(p, rho);
-    return sqrt(R(2.0) * (pr - cs2 * rho) / (cs2 * R(p.G)));
+    const R pr = pressure_of<R>(p, rho);
+    return sqrt(rdiv(rmul(R(2.0), rsub(pr, rmul(cs2, rho))), rmul(cs2, R(p.G))));
   }
-  return R(1.0) - expr(-rho);
+  return rsub(R(1.0), expr(-rho));
 }
 
 // 0: interior fluid node, 1: inlet slab, 2: outlet slab (drainage boundary,
@@ -169,11 +183,11 @@ __device__ __forceinline__ R inject(const Phys& p, const Geom& g,
   if (p.rho_inject_period != 0 &&
       (float)y < p.inject_position * (float)g.ly &&
       (unsigned long long)s.step % p.rho_inject_period == 0ull) {
-    const R inc = R(p.rho_increment) * R(s.reverse);
+    const R inc = rmul(R(p.rho_increment), R(s.reverse));
     switch (s.inject_type) {
-      case 0: d += inc; break;
-      case 1: if (d < R(p.rhol_spinodal)) d += inc; break;
-      case 2: if (d > R(p.rhol_spinodal)) d += inc; break;
+      case 0: d = radd(d, inc); break;
+      case 1: if (d < R(p.rhol_spinodal)) d = radd(d, inc); break;
+      case 2: if (d > R(p.rhol_spinodal)) d = radd(d, inc); break;
       default: break;
     }
   }
