@@ -180,8 +180,9 @@ mlbm_status mlbm_iterate(mlbm_lattice* lat, int64_t step0, int32_t nsteps,
 #define MLBM_KERNEL_FUSED 1
 #define MLBM_KERNEL_TWO_PASS 2
 mlbm_status mlbm_set_step_kernel(mlbm_lattice* lat, int32_t kind);
-/* Tuning of the fused kernel: rows per work item (0 = automatic) and the
- * plane lag between a plane's density pass and its update pass (0 = 4). */
+/* Tuning of the fused kernel: tile rows (the tile is 32 x rows nodes of an
+ * (x, y) plane; 0 = automatic, else 1, 2, 4, 8 or 16) and the lag in planes
+ * between a plane's density pass and its update pass (0 = 4, at least 2). */
 mlbm_status mlbm_set_tuning(mlbm_lattice* lat, int32_t rows_per_item,
                             int32_t plane_lag);
 /* Wait for the lattice's stream and report a device-side failure (a bounded

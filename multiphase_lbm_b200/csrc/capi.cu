@@ -241,7 +241,7 @@ mlbm_status check_device_error(mlbm_lattice* lat) {
            "error flag read");
   if (!h) return MLBM_OK;
   cudaMemset(lat->err, 0, sizeof(int));
-  cudaMemset(lat->pdone, 0, sizeof(unsigned) * lat->g.lz);
+  cudaMemset(lat->pdone, 0, sizeof(unsigned) * max_tiles(lat->g));
   lat->fused_epoch = 0;
   lat->initialized = false;
   return fail(MLBM_ERR_TIMEOUT,
@@ -343,9 +343,10 @@ mlbm_status mlbm_lattice_create(int32_t lx, int32_t ly, int32_t lz,
   alloc((void**)&lat->mask, mask_words * sizeof(uint32_t));
   alloc((void**)&lat->vel, np * 3 * sizeof(float));
   alloc((void**)&lat->nbw, np * sizeof(uint32_t));
-  alloc((void**)&lat->pdone, (size_t)lz * sizeof(unsigned));
+  const size_t ncount = (size_t)max_tiles(lat->g);
+  alloc((void**)&lat->pdone, ncount * sizeof(unsigned));
   alloc((void**)&lat->err, sizeof(int));
-  if (e == cudaSuccess) e = cudaMemset(lat->pdone, 0, (size_t)lz * sizeof(unsigned));
+  if (e == cudaSuccess) e = cudaMemset(lat->pdone, 0, ncount * sizeof(unsigned));
   if (e == cudaSuccess) e = cudaMemset(lat->err, 0, sizeof(int));
   if (e == cudaSuccess) e = cudaMemset(lat->mask, 0, mask_words * 4);
   if (e == cudaSuccess) e = cudaMemset(lat->rho_init, 0, np * sizeof(float));
@@ -641,17 +642,16 @@ mlbm_status mlbm_set_step_kernel(mlbm_lattice* lat, int32_t kind) {
 mlbm_status mlbm_set_tuning(mlbm_lattice* lat, int32_t rows_per_item,
                             int32_t plane_lag) {
   if (mlbm_status st = check_lat(lat)) return st;
-  if (rows_per_item < 0 || plane_lag < 0 || rows_per_item > 512)
-    return fail(MLBM_ERR_ARG, "invalid tuning");
-  const FusedShape f = fused_shape(lat->g, lat->storage, rows_per_item, plane_lag);
-  if (!f.ok) return fail(MLBM_ERR_ARG, "tuning does not fit the fused kernel");
+  if (rows_per_item < 0 || plane_lag < 0 || rows_per_item > 16 ||
+      (rows_per_item & (rows_per_item - 1)) != 0 || plane_lag > 64)
+    return fail(MLBM_ERR_ARG, "invalid tuning (rows 0 or 1..16 power of two, lag 0..64)");
   if (mlbm_status st = activate(lat)) return st;
-  // the per-plane counters count items, so a new item size restarts them
+  // the progress counters count this tiling's planes: restart them
   CUDA_TRY(cudaStreamSynchronize(lat->stream), "tuning sync");
-  CUDA_TRY(cudaMemset(lat->pdone, 0, sizeof(unsigned) * lat->g.lz), "counter reset");
-  lat->fused = f;
+  CUDA_TRY(cudaMemset(lat->pdone, 0, sizeof(unsigned) * max_tiles(lat->g)),
+           "counter reset");
+  lat->fused = fused_shape(lat->g, lat->storage, rows_per_item, plane_lag);
   lat->fused_epoch = 0;
-  for (int& v : lat->fused_grid) v = 0;
   return MLBM_OK;
 }
 

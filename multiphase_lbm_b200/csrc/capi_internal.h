@@ -10,9 +10,10 @@
 namespace mlbm {
 // Launch geometry of the fused persistent time step (persistent.cuh).
 struct FusedShape {
-  int W, nseg, By, threads, rb_y, R, L;
+  int Tx, Ty, ntx, nty, ntiles, threads, L;
   size_t smem;
-  bool ok;  // fits (shared memory, threads); otherwise the two-pass kernels
+  bool ok;      // false: the fused kernel cannot run this lattice
+  bool chosen;  // tile shape fixed (by tuning or at the first launch)
 };
 }  // namespace mlbm
 
@@ -39,9 +40,8 @@ struct mlbm_lattice {
 
   // fused persistent step
   mlbm::FusedShape fused{};
-  int fused_grid[6] = {0, 0, 0, 0, 0, 0};  // per (phase, output) variant
-  unsigned long long fused_epoch = 0;      // launches since counter reset
-  unsigned* pdone = nullptr;               // per-plane completion counters
+  unsigned long long fused_epoch = 0;      // progress-counter base
+  unsigned* pdone = nullptr;               // per-tile progress counters
   int* err = nullptr;                      // device error flag (wait timeout)
   int step_kernel = 0;                     // MLBM_KERNEL_*
 
@@ -56,7 +56,8 @@ mlbm_status cuda_fail(cudaError_t e, const char* where);
 size_t pop_elem_bytes(int storage);
 size_t real_bytes(int storage);
 Geom make_geom(int lx, int ly, int lz);
-FusedShape fused_shape(const Geom& g, int storage, int by_hint, int lag);
+FusedShape fused_shape(const Geom& g, int storage, int ty_hint, int lag);
+int max_tiles(const Geom& g);
 struct StepArgs;
 template <typename T>
 mlbm_status launch_fused(mlbm_lattice* lat, const StepArgs& a, int out);

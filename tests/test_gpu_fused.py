@@ -59,7 +59,7 @@ def test_fused_storage_formats(storage):
         assert np.array_equal(u, v)
 
 
-@pytest.mark.parametrize("tuning", [(1, 2), (3, 2), (2, 7), (8, 50)])
+@pytest.mark.parametrize("tuning", [(1, 2), (2, 3), (4, 7), (16, 50)])
 def test_fused_tuning_variants(tuning):
     from multiphase_lbm_b200 import capi
     shape = (64, 21, 13)
