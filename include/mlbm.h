@@ -83,7 +83,7 @@ typedef enum mlbm_dtype { MLBM_DTYPE_F32 = 0, MLBM_DTYPE_F64 = 1,
  * (include/iteration_host.h:30-41, defaults src/multiphase_lbm.cu:35-80) plus
  * the drainage boundary, which the reference does not have: fluid nodes with
  * x < inlet_width are held at rho_inlet and fluid nodes with
- * x >= lx - outlet_width at rho_outlet (density fixed, post-collision
+ * x >= nx - outlet_width at rho_outlet (density fixed, post-collision
  * populations the rest equilibrium t_i * rho).  Both widths 0 = periodic. */
 typedef struct mlbm_params {
   float tau;
@@ -135,14 +135,14 @@ const char* mlbm_last_error(void);
  * w[19] (include/lbm_model.cuh:35-54). */
 void mlbm_d3q19(int32_t* e, float* w);
 
-/* Create a lattice of lx*ly*lz nodes on `device` with the given storage.
+/* Create a lattice of nx*ny*nz nodes on `device` with the given storage.
  * Allocates all device memory up front (MLBM_ERR_NOMEM if refused). */
-mlbm_status mlbm_lattice_create(int32_t lx, int32_t ly, int32_t lz,
+mlbm_status mlbm_lattice_create(int32_t nx, int32_t ny, int32_t nz,
                                 int32_t storage, int32_t device,
                                 mlbm_lattice** out);
 mlbm_status mlbm_lattice_destroy(mlbm_lattice* lat);
 /* Device bytes held by a lattice of this size and storage (no allocation). */
-uint64_t mlbm_lattice_bytes(int32_t lx, int32_t ly, int32_t lz,
+uint64_t mlbm_lattice_bytes(int32_t nx, int32_t ny, int32_t nz,
                             int32_t storage);
 
 /* CUDA stream (cudaStream_t) the lattice's work is issued on; NULL = the
@@ -192,7 +192,7 @@ mlbm_status mlbm_synchronize(mlbm_lattice* lat);
 
 /* Copy a field out in the reference layout.  dtype: MLBM_DTYPE_F32 or
  * MLBM_DTYPE_F64 (F64 keeps an FP64 lattice's full precision), U8 for
- * MLBM_FIELD_FLUID.  host_out: lx*ly*lz*components elements.  Synchronous. */
+ * MLBM_FIELD_FLUID.  host_out: nx*ny*nz*components elements.  Synchronous. */
 mlbm_status mlbm_download_field(mlbm_lattice* lat, int32_t field,
                                 int32_t dtype, void* host_out);
 /* Same into device memory (stream-ordered, no synchronisation). */
@@ -202,7 +202,7 @@ mlbm_status mlbm_download_field_device(mlbm_lattice* lat, int32_t field,
 /* Phase statistics of the current state (device reduction, deterministic).
  * Synchronous. */
 mlbm_status mlbm_phase_stats(mlbm_lattice* lat, mlbm_stats* out);
-/* Per-x-plane counts of fluid and liquid nodes (int64[lx] each).  Sync. */
+/* Per-x-plane counts of fluid and liquid nodes (int64[nx] each).  Sync. */
 mlbm_status mlbm_plane_profile(mlbm_lattice* lat, int64_t* n_fluid_x,
                                int64_t* n_liquid_x);
 
@@ -216,15 +216,15 @@ mlbm_status mlbm_plane_profile(mlbm_lattice* lat, int64_t* n_fluid_x,
  * (z fastest); the EOS and thresholds come from *params.  Runs on `stream`
  * (NULL = legacy default) and waits for it; *out is host memory.
  * Its scratch is a fixed static device array (about 459 KB on every GPU that
- * loads the library, kept until exit), so lx may not exceed
+ * loads the library, kept until exit), so nx may not exceed
  * MLBM_NOALLOC_MAX_LX (MLBM_ERR_ARG otherwise).  The first call on each
  * device looks up the array's device address; make it before any stream
  * capture starts.  Calls share the array: calls that overlap on the GPU race
  * and must be serialised by the caller. */
 #define MLBM_NOALLOC_MAX_LX 4096
 mlbm_status mlbm_phase_stats_noalloc(const float* rho_dev,
-                                     const uint8_t* is_fluid_dev, int32_t lx,
-                                     int32_t ly, int32_t lz,
+                                     const uint8_t* is_fluid_dev, int32_t nx,
+                                     int32_t ny, int32_t nz,
                                      const mlbm_params* params, void* stream,
                                      mlbm_stats* out);
 

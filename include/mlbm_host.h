@@ -31,7 +31,7 @@ extern "C" {
  * strictly inside (float distance^2 < R^2) marks node floor(p + 0.5), wrapped
  * once periodically.  solid_number (optional, may be NULL) receives `id`. */
 mlbm_status mlbm_place_sphere(uint8_t* is_fluid, int64_t* solid_number,
-                              int32_t lx, int32_t ly, int32_t lz, float x,
+                              int32_t nx, int32_t ny, int32_t nz, float x,
                               float y, float z, float R, int64_t id);
 
 /* Read a positions file (one value per line: x, y, z, r per grain, each
@@ -39,22 +39,22 @@ mlbm_status mlbm_place_sphere(uint8_t* is_fluid, int64_t* solid_number,
  * number of grains; solid ids continue from *count on entry. */
 mlbm_status mlbm_read_positions(const char* path, float resolution,
                                 uint8_t* is_fluid, int64_t* solid_number,
-                                int32_t lx, int32_t ly, int32_t lz,
+                                int32_t nx, int32_t ny, int32_t nz,
                                 int64_t* count);
 
 /* rho = rho0 * (1 + rate * (rand()/RAND_MAX - 0.5)) after srand(1), loop
  * order z, y, x (the C library's rand(), as the reference). */
-mlbm_status mlbm_init_density(float* rho, int32_t lx, int32_t ly, int32_t lz,
+mlbm_status mlbm_init_density(float* rho, int32_t nx, int32_t ny, int32_t nz,
                               float rho0, float rate);
 
-/* Seeded packing: spheres with centres uniform in [0,lx)x[0,ly)x[0,lz) and
+/* Seeded packing: spheres with centres uniform in [0,nx)x[0,ny)x[0,nz) and
  * radius uniform in [rmin, rmax] (splitmix64 stream from `seed`, overlap
  * allowed) are added until the porosity is <= porosity_target or
  * max_spheres are placed.  is_fluid must be all 1 on entry (it is reset).
  * xyzr (optional, 4 floats per sphere, capacity max_spheres) receives the
  * spheres in positions-file order; *count the number placed; *porosity the
  * final porosity. */
-mlbm_status mlbm_generate_packing(int32_t lx, int32_t ly, int32_t lz,
+mlbm_status mlbm_generate_packing(int32_t nx, int32_t ny, int32_t nz,
                                   float rmin, float rmax,
                                   double porosity_target, uint64_t seed,
                                   int64_t max_spheres, uint8_t* is_fluid,
@@ -63,7 +63,7 @@ mlbm_status mlbm_generate_packing(int32_t lx, int32_t ly, int32_t lz,
 
 /* The reference's generate_solids: `num` grains from the C library rand(). */
 mlbm_status mlbm_generate_solids(uint8_t* is_fluid, int64_t* solid_number,
-                                 int32_t lx, int32_t ly, int32_t lz,
+                                 int32_t nx, int32_t ny, int32_t nz,
                                  int32_t num, float rmin, float rmax,
                                  float xmin, float xmax, float ymin,
                                  float ymax, float zmin, float zmax,
@@ -74,13 +74,13 @@ mlbm_status mlbm_write_positions(const char* path, const float* xyzr,
                                  int64_t count);
 
 /* Fraction of solid nodes. */
-double mlbm_packing_density(const uint8_t* is_fluid, int32_t lx, int32_t ly,
-                            int32_t lz);
+double mlbm_packing_density(const uint8_t* is_fluid, int32_t nx, int32_t ny,
+                            int32_t nz);
 
 /* Read the "SCALARS Density" block of a legacy VTK file written by
  * mlbm_write_vtk (or the reference's write_vtk_ascii) into rho. */
-mlbm_status mlbm_read_density_vtk(const char* path, float* rho, int32_t lx,
-                                  int32_t ly, int32_t lz);
+mlbm_status mlbm_read_density_vtk(const char* path, float* rho, int32_t nx,
+                                  int32_t ny, int32_t nz);
 
 #ifdef __cplusplus
 }

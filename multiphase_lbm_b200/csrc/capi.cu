@@ -437,7 +437,7 @@ mlbm_status mlbm_upload_fluid_mask(mlbm_lattice* lat, const uint8_t* f) {
   if (mlbm_status st = check_lat(lat)) return st;
   if (!f) return fail(MLBM_ERR_ARG, "null mask");
   if (mlbm_status st = activate(lat)) return st;
-  return upload_mask_impl(lat, f, cudaMemcpyHostToDevice);
+  return upload_mask_impl(lat, f, cudaMemcpyDefault);
 }
 mlbm_status mlbm_upload_fluid_mask_device(mlbm_lattice* lat, const uint8_t* f) {
   if (mlbm_status st = check_lat(lat)) return st;
@@ -449,7 +449,7 @@ mlbm_status mlbm_upload_rho(mlbm_lattice* lat, const float* r) {
   if (mlbm_status st = check_lat(lat)) return st;
   if (!r) return fail(MLBM_ERR_ARG, "null rho");
   if (mlbm_status st = activate(lat)) return st;
-  return upload_rho_impl(lat, r, cudaMemcpyHostToDevice);
+  return upload_rho_impl(lat, r, cudaMemcpyDefault);
 }
 mlbm_status mlbm_upload_rho_device(mlbm_lattice* lat, const float* r) {
   if (mlbm_status st = check_lat(lat)) return st;
@@ -529,8 +529,9 @@ mlbm_status mlbm_download_field(mlbm_lattice* lat, int32_t field,
   if (mlbm_status st = ensure_staging(lat, bytes)) return st;
   if (mlbm_status st = mlbm_download_field_device(lat, field, dtype, lat->staging))
     return st;
-  CUDA_TRY(cudaMemcpyAsync(host_out, lat->staging, bytes,
-                           cudaMemcpyDeviceToHost, lat->stream),
+  // cudaMemcpyDefault: host_out may be pageable, pinned or managed memory
+  CUDA_TRY(cudaMemcpyAsync(host_out, lat->staging, bytes, cudaMemcpyDefault,
+                           lat->stream),
            "field download copy");
   CUDA_TRY(cudaStreamSynchronize(lat->stream), "field download");
   return check_device_error(lat);

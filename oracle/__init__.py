@@ -65,6 +65,7 @@ def build() -> None:
     subprocess.run(["make", "-s", "-C", HERE], check=True)
     from . import build_ref  # noqa: WPS433
     build_ref.build()
+    build_ref.build_dropin(["40x40x40"])
 
 
 def _load(path: str) -> C.CDLL:
@@ -156,6 +157,9 @@ class Reference:
                                             C.c_void_p, C.c_void_p]
             lib.ref_driver_stats.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p,
                                              C.c_float, C.c_float, C.c_void_p]
+            lib.ref_driver_clusters.argtypes = [
+                C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64,
+                C.c_float, C.c_float, C.c_void_p, C.c_void_p, C.c_void_p]
             Reference._libs[shape] = lib
         self.lib = Reference._libs[shape]
         self.shape = shape
@@ -207,3 +211,23 @@ class Reference:
                 "liq_clusters", "gas_clusters", "min_rho", "max_rho", "min_p",
                 "max_p"]
         return dict(zip(keys, out.tolist()))
+
+    def driver_clusters(self, rho, pressure, fluid, solid_number, solid_count,
+                        rhol, rhog):
+        """Run the reference calc_cluster (with solid numbers): returns
+        (dict of cluster columns, liquid labels, gas labels)."""
+        out = np.zeros(8, np.float64)
+        liq = np.zeros(self.shape, np.int64)
+        gas = np.zeros(self.shape, np.int64)
+        r = np.ascontiguousarray(rho, np.float32)
+        p = np.ascontiguousarray(pressure, np.float32)
+        f = np.ascontiguousarray(fluid, np.uint8)
+        sn = np.ascontiguousarray(solid_number, np.int64)
+        self.lib.ref_driver_clusters(r.ctypes.data, p.ctypes.data, f.ctypes.data,
+                                     sn.ctypes.data, solid_count, rhol, rhog,
+                                     out.ctypes.data, liq.ctypes.data,
+                                     gas.ctypes.data)
+        keys = ["liq_cluster_count", "gas_cluster_count", "cluster_order",
+                "wet_coord_num", "cluster_radius", "liquid_solid_boundary",
+                "liquid_vapor_boundary", "saturation"]
+        return dict(zip(keys, out.tolist())), liq, gas

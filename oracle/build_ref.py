@@ -108,12 +108,64 @@ def build(sizes=None, force: bool = False, quiet: bool = True) -> list[str]:
     return built
 
 
+# The reference's own host driver (src/multiphase_lbm.cu, src/main.cc)
+# linked against libmlbm through include/mlbm_compat.h instead of its CUDA
+# kernels: the drop-in demonstration.  Its iteration_host.h is replaced by a
+# generated three-line header that includes mlbm_compat.h.
+COMPAT_HEADER = """#ifndef ITERATION_HOST_H_
+#define ITERATION_HOST_H_
+#include <cuda_runtime.h>
+#include "lbm_model.cuh"
+#include "mlbm_compat.h"
+#define cudaErrorCheck(ans) { mlbm_compat_check((int)(ans), __FILE__, __LINE__); }
+#endif
+"""
+
+
+def build_dropin(sizes=None, force: bool = False) -> list[str]:
+    """Build oracle/_ref/refdriver_b200_<size>: the reference driver running
+    the B200 kernels (needs libmlbm.so built first)."""
+    if not os.path.isdir(os.path.join(REFERENCE, "include")):
+        return []
+    root_repo = os.path.dirname(HERE)
+    lib = os.path.join(root_repo, "multiphase_lbm_b200", "libmlbm.so")
+    if not os.path.exists(lib):
+        return []
+    nvcc = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+    scratch = os.path.join(tempfile.gettempdir(), "mlbm_ref_build")
+    out = []
+    for size in sizes or SIZES:
+        exe = os.path.join(OUT, f"refdriver_b200_{size}")
+        if (not force and os.path.exists(exe)
+                and os.path.getmtime(exe) > os.path.getmtime(lib)):
+            out.append(exe)
+            continue
+        root = _prepare_tree(size, scratch)
+        gen = os.path.join(root, "compat_include")
+        os.makedirs(gen, exist_ok=True)
+        with open(os.path.join(gen, "iteration_host.h"), "w") as fh:
+            fh.write(COMPAT_HEADER)
+        cmd = [nvcc, "-O2", "-std=c++14", "-w", "-Xcompiler", "-fopenmp",
+               "-I", gen, "-I", os.path.join(root, "include"),
+               "-I", os.path.join(root, "external"),
+               "-I", os.path.join(root_repo, "include"),
+               os.path.join(root, "src", "multiphase_lbm.cu"),
+               os.path.join(root, "src", "main.cc"),
+               "-L", os.path.dirname(lib), "-lmlbm",
+               "-Xlinker", "-rpath,$ORIGIN/../../multiphase_lbm_b200",
+               "-o", exe]
+        subprocess.run(cmd, check=True)
+        out.append(exe)
+    return out
+
+
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
     ap.add_argument("--sizes", default=",".join(SIZES))
     ap.add_argument("--force", action="store_true")
     args = ap.parse_args(argv)
     libs = build(args.sizes.split(","), force=args.force, quiet=False)
+    libs += build_dropin(args.sizes.split(","), force=args.force)
     if not libs:
         print("reference sources not present; nothing built")
     return 0

@@ -297,6 +297,11 @@ int ref_driver_stats(const float* rho, const float* pressure,
   box->IniPerturbRate = 0.f;
   box->resize_gpu();
   const size_t n = (size_t)lx * ly * lz;
+  // resize_gpu never initialises the gas-cluster arrays (src/multiphase_lbm.cu
+  // :146-156) and calc_cluster resets them at fluid nodes only, so the gas
+  // flood would read uninitialised memory at solid nodes; start them at zero.
+  std::memset(box->gas_cluster, 0, n * sizeof(bool));
+  std::memset(box->gas_cluster_number, 0, n * sizeof(size_t));
   std::memcpy(box->drho, rho, n * sizeof(real));
   std::memcpy(box->dpressure, pressure, n * sizeof(real));
   bool* fl = (bool*)box->dis_fluid;
@@ -328,6 +333,57 @@ int ref_driver_stats(const float* rho, const float* pressure,
   out[11] = pmn;
   out[12] = pmx;
   std::free(box->dsolid_touch_liquid);  // the reference destructor leaks it
+  delete box;
+  return 0;
+}
+
+// calc_cluster with solid numbers (cluster order, wet coordination number,
+// single-cluster radius): out = {liq_cluster_count, gas_cluster_count,
+// cluster_order, wet_coord_num, max_r, ratio_liquid_solid_boundary,
+// ratio_liquid_vapor_boundary, saturation}; liq/gas labels copied out.
+int ref_driver_clusters(const float* rho, const float* pressure,
+                        const uint8_t* fluid, const int64_t* solid_number,
+                        int64_t solid_count, float rhol, float rhog,
+                        double* out, int64_t* liq_labels, int64_t* gas_labels) {
+  MultiphaseLBM* box = new MultiphaseLBM();
+  box->rho0 = 1.f;
+  box->IniPerturbRate = 0.f;
+  box->resize_gpu();
+  const size_t n = (size_t)lx * ly * lz;
+  // resize_gpu never initialises the gas-cluster arrays (src/multiphase_lbm.cu
+  // :146-156) and calc_cluster resets them at fluid nodes only, so the gas
+  // flood would read uninitialised memory at solid nodes; start them at zero.
+  std::memset(box->gas_cluster, 0, n * sizeof(bool));
+  std::memset(box->gas_cluster_number, 0, n * sizeof(size_t));
+  std::memcpy(box->drho, rho, n * sizeof(real));
+  std::memcpy(box->dpressure, pressure, n * sizeof(real));
+  bool* fl = (bool*)box->dis_fluid;
+  size_t* sn = (size_t*)box->solid_number;
+  for (size_t k = 0; k < n; ++k) {
+    fl[k] = fluid[k] != 0;
+    sn[k] = (size_t)solid_number[k];
+  }
+  box->solid_count = (size_t)solid_count;
+  box->rhol_spinodal = rhol;
+  box->rhog_spinodal = rhog;
+  box->vtkPeriod = 1u << 30;
+  box->step = 1;
+  box->calc_cluster();
+  out[0] = (double)box->liq_cluster_count;
+  out[1] = (double)box->gas_cluster_count;
+  out[2] = box->cluster_order;
+  out[3] = box->wet_coord_num;
+  out[4] = box->max_r;
+  out[5] = box->ratio_liquid_solid_boundary;
+  out[6] = box->ratio_liquid_vapor_boundary;
+  out[7] = box->saturation_ratio;
+  const size_t* ll = (const size_t*)box->liq_cluster_number;
+  const size_t* gl = (const size_t*)box->gas_cluster_number;
+  for (size_t k = 0; k < n; ++k) {
+    liq_labels[k] = (int64_t)ll[k];
+    gas_labels[k] = (int64_t)gl[k];
+  }
+  std::free(box->dsolid_touch_liquid);
   delete box;
   return 0;
 }
