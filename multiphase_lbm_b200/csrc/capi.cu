@@ -8,6 +8,7 @@
 
 #include <cstdarg>
 #include <cstdio>
+#include <algorithm>
 #include <cstring>
 #include <new>
 #include <string>
@@ -17,6 +18,7 @@
 #include "io_kernels.cuh"
 #include "kernels.cuh"
 #include "persistent.cuh"
+#include "update_tma.cuh"
 
 using namespace mlbm;
 
@@ -62,7 +64,54 @@ Geom make_geom(int lx, int ly, int lz) {
   g.px = (lx + 31) / 32 * 32;
   g.wpr = g.px / 32;
   g.plane = (long long)lz * ly * g.px;
+  g.pxg = g.px + 8;
   return g;
+}
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link
+// dependency on libcuda).
+mlbm_status setup_update(mlbm_lattice* lat, int rows, int planes) {
+  using Encode = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t,
+                              void*, const cuuint64_t*, const cuuint64_t*,
+                              const cuuint32_t*, const cuuint32_t*,
+                              CUtensorMapInterleave, CUtensorMapSwizzle,
+                              CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+  static Encode encode = nullptr;
+  if (!encode) {
+    void* fn = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault,
+                                &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess || !fn) {
+      cudaGetLastError();
+      return set_error(MLBM_ERR_CUDA, "cuTensorMapEncodeTiled not available");
+    }
+    encode = reinterpret_cast<Encode>(fn);
+  }
+  const Geom& g = lat->g;
+  ZMarch& zm = lat->zm;
+  zm.By = std::max(1, std::min(rows, 8));
+  zm.Dz = std::max(1, planes);
+  zm.ntx = g.px / 32;
+  zm.nty = (g.ly + zm.By - 1) / zm.By;
+  zm.nzc = (g.lz + zm.Dz - 1) / zm.Dz;
+  const bool f64 = lat->storage == MLBM_STORE_F64;
+  const size_t esz = f64 ? 8 : 4;
+  cuuint64_t dims[3] = {(cuuint64_t)g.pxg, (cuuint64_t)(g.ly + 2),
+                        (cuuint64_t)(g.lz + 2)};
+  cuuint64_t strides[2] = {(cuuint64_t)g.pxg * esz,
+                           (cuuint64_t)g.pxg * (g.ly + 2) * esz};
+  cuuint32_t box[3] = {(cuuint32_t)kBoxX, (cuuint32_t)(zm.By + 2), 1};
+  cuuint32_t estr[3] = {1, 1, 1};
+  const CUresult r = encode(
+      &lat->psi_map,
+      f64 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3,
+      lat->psi, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+      CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+      CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS)
+    return set_error(MLBM_ERR_CUDA, "psi tensor map could not be encoded");
+  return MLBM_OK;
 }
 
 }  // namespace mlbm
@@ -97,6 +146,7 @@ Phys to_phys(const mlbm_params& p) {
   q.rho_inlet = p.rho_inlet;
   q.rho_outlet = p.rho_outlet;
   q.rho_shift = p.rho_shift;
+  q.omega = (float)(1.0 / (double)p.tau);
   return q;
 }
 
@@ -110,40 +160,50 @@ mlbm_status activate(const mlbm_lattice* lat) {
   return MLBM_OK;
 }
 
-template <typename T>
-mlbm_status launch_two_pass(mlbm_lattice* lat, const StepArgs& a, bool wu) {
+template <typename T, int PHASE>
+void launch_density(mlbm_lattice* lat, const StepArgs& a, bool write_rho) {
   using R = typename Pop<T>::Real;
-  T* pop = static_cast<T*>(lat->pop);
+  const T* pop = static_cast<const T*>(lat->pop);
   R* rho = static_cast<R*>(lat->rho);
   R* psi = static_cast<R*>(lat->psi);
-  const dim3 grid = node_grid(lat->g), block = node_block();
+  if (write_rho)
+    k_density<T, PHASE, true><<<node_grid(lat->g), node_block(), 0, lat->stream>>>(
+        pop, lat->nbw, rho, psi, lat->g, lat->phys, a);
+  else
+    k_density<T, PHASE, false><<<node_grid(lat->g), node_block(), 0, lat->stream>>>(
+        pop, lat->nbw, rho, psi, lat->g, lat->phys, a);
+}
+
+template <typename T, int PHASE, bool WU>
+void launch_update(mlbm_lattice* lat, const StepArgs& a) {
+  using R = typename Pop<T>::Real;
+  const ZMarch& zm = lat->zm;
+  const size_t smem = update_smem_bytes(zm.By, sizeof(R));
+  k_update_zm<T, PHASE, WU>
+      <<<zm.ntx * zm.nty * zm.nzc, 32 * zm.By, smem, lat->stream>>>(
+          static_cast<T*>(lat->pop), lat->nbw, lat->vel, lat->err, lat->g,
+          lat->phys, a, zm, lat->psi_map);
+}
+
+template <typename T>
+mlbm_status launch_two_pass(mlbm_lattice* lat, const StepArgs& a, bool wu,
+                            bool write_rho) {
   if (lat->phase == 0) {
-    k_density<T, 0><<<grid, block, 0, lat->stream>>>(pop, lat->nbw, rho, psi,
-                                                     lat->g, lat->phys, a);
-    if (wu)
-      k_update<T, 0, true><<<grid, block, 0, lat->stream>>>(
-          pop, lat->nbw, rho, psi, lat->vel, lat->g, lat->phys, a);
-    else
-      k_update<T, 0, false><<<grid, block, 0, lat->stream>>>(
-          pop, lat->nbw, rho, psi, lat->vel, lat->g, lat->phys, a);
+    launch_density<T, 0>(lat, a, write_rho);
+    if (wu) launch_update<T, 0, true>(lat, a);
+    else launch_update<T, 0, false>(lat, a);
   } else {
-    k_density<T, 1><<<grid, block, 0, lat->stream>>>(pop, lat->nbw, rho, psi,
-                                                     lat->g, lat->phys, a);
-    if (wu)
-      k_update<T, 1, true><<<grid, block, 0, lat->stream>>>(
-          pop, lat->nbw, rho, psi, lat->vel, lat->g, lat->phys, a);
-    else
-      k_update<T, 1, false><<<grid, block, 0, lat->stream>>>(
-          pop, lat->nbw, rho, psi, lat->vel, lat->g, lat->phys, a);
+    launch_density<T, 1>(lat, a, write_rho);
+    if (wu) launch_update<T, 1, true>(lat, a);
+    else launch_update<T, 1, false>(lat, a);
   }
   CUDA_TRY(cudaGetLastError(), "time-step launch");
   return MLBM_OK;
 }
 
 // One lattice step per launch (two launches for the two-pass kernels, which
-// AUTO selects).  The fused persistent kernel writes rho only when asked (the
-// last step of each mlbm_iterate call); the two-pass kernels write it every
-// step.
+// AUTO selects).  rho is written on the last step of each mlbm_iterate call
+// (the field the caller can read afterwards).
 template <typename T>
 mlbm_status launch_steps(mlbm_lattice* lat, int64_t step0, int32_t nsteps,
                          int32_t reverse, uint32_t inject_type,
@@ -159,7 +219,7 @@ mlbm_status launch_steps(mlbm_lattice* lat, int64_t step0, int32_t nsteps,
     if (fused)
       st = launch_fused<T>(lat, a, wu ? (OUT_RHO | OUT_VEL) : (last ? OUT_RHO : OUT_NONE));
     else
-      st = launch_two_pass<T>(lat, a, wu);
+      st = launch_two_pass<T>(lat, a, wu, last);
     if (st) return st;
     lat->phase ^= 1;
     if (wu) lat->vel_valid = true;
@@ -299,7 +359,8 @@ uint64_t mlbm_lattice_bytes(int32_t lx, int32_t ly, int32_t lz,
   const Geom g = make_geom(lx, ly, lz);
   const uint64_t np = (uint64_t)g.plane;
   return np * Q * pop_elem_bytes(storage)     // populations
-         + 2 * np * real_bytes(storage)       // rho, psi
+         + np * real_bytes(storage)           // rho
+         + (uint64_t)psi_elems(g) * real_bytes(storage)  // psi with ghosts
          + np * 4                             // initial density
          + (uint64_t)g.lz * g.ly * g.wpr * 4  // mask
          + np * 12                            // velocity
@@ -338,7 +399,7 @@ mlbm_status mlbm_lattice_create(int32_t lx, int32_t ly, int32_t lz,
   };
   alloc(&lat->pop, np * Q * pop_elem_bytes(storage));
   alloc(&lat->rho, np * real_bytes(storage));
-  alloc(&lat->psi, np * real_bytes(storage));
+  alloc(&lat->psi, (size_t)psi_elems(lat->g) * real_bytes(storage));
   alloc((void**)&lat->rho_init, np * sizeof(float));
   alloc((void**)&lat->mask, mask_words * sizeof(uint32_t));
   alloc((void**)&lat->vel, np * 3 * sizeof(float));
@@ -347,6 +408,8 @@ mlbm_status mlbm_lattice_create(int32_t lx, int32_t ly, int32_t lz,
   alloc((void**)&lat->pdone, ncount * sizeof(unsigned));
   alloc((void**)&lat->err, sizeof(int));
   if (e == cudaSuccess) e = cudaMemset(lat->pdone, 0, ncount * sizeof(unsigned));
+  if (e == cudaSuccess)
+    e = cudaMemset(lat->psi, 0, (size_t)psi_elems(lat->g) * real_bytes(storage));
   if (e == cudaSuccess) e = cudaMemset(lat->err, 0, sizeof(int));
   if (e == cudaSuccess) e = cudaMemset(lat->mask, 0, mask_words * 4);
   if (e == cudaSuccess) e = cudaMemset(lat->rho_init, 0, np * sizeof(float));
@@ -354,6 +417,10 @@ mlbm_status mlbm_lattice_create(int32_t lx, int32_t ly, int32_t lz,
     mlbm_lattice_destroy(lat);
     cudaGetLastError();
     return cuda_fail(e, "lattice allocation");
+  }
+  if (mlbm_status st = setup_update(lat, 4, 16)) {
+    mlbm_lattice_destroy(lat);
+    return st;
   }
   *out = lat;
   return MLBM_OK;

@@ -1,11 +1,13 @@
 // capi_internal.h -- the lattice handle behind the C ABI (not exported).
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include "../../include/mlbm.h"
 #include "errors.h"
 #include "lattice.cuh"
+#include "update_tma.cuh"
 
 namespace mlbm {
 // Launch geometry of the fused persistent time step (persistent.cuh).
@@ -38,6 +40,10 @@ struct mlbm_lattice {
   double* stats_scratch = nullptr;
   size_t stats_scratch_bytes = 0;
 
+  // update pass: z-march tiles and the TMA descriptor of the psi tensor
+  mlbm::ZMarch zm{};
+  alignas(64) CUtensorMap psi_map;
+
   // fused persistent step
   mlbm::FusedShape fused{};
   unsigned long long fused_epoch = 0;      // progress-counter base
@@ -58,6 +64,8 @@ size_t real_bytes(int storage);
 Geom make_geom(int lx, int ly, int lz);
 FusedShape fused_shape(const Geom& g, int storage, int ty_hint, int lag);
 int max_tiles(const Geom& g);
+// (Re)build the update pass's tile shape and psi tensor map.
+mlbm_status setup_update(mlbm_lattice* lat, int rows, int planes);
 struct StepArgs;
 template <typename T>
 mlbm_status launch_fused(mlbm_lattice* lat, const StepArgs& a, int out);

@@ -142,24 +142,33 @@ __device__ __forceinline__ void collide(const Phys& p, R d, R psi_self,
     if (ez(i)) uz = ez(i) > 0 ? radd(uz, f[i]) : rsub(uz, f[i]);
   }
   const R tau = R(p.tau);
-  const R inv_rho = rdiv(R(1), d);
+  const R inv_rho = rrcp(d);
   ux = rmul(rfma(tau, Fx, ux), inv_rho);
   uy = rmul(rfma(tau, Fy, uy), inv_rho);
   uz = rmul(rfma(tau, Fz, uz), inv_rho);
   const R usq15 =
       rmul(R(1.5), rfma(uz, uz, rfma(uy, uy, rmul(ux, ux))));
-  const R omega = rdiv(R(1), tau);
+  const R omega = R(p.omega);
   // BGK, include/iteration_device.cuh:162-174:
   //   f_i += (t_i rho (1 + 3 eu + 4.5 eu^2 - 1.5 u^2) - f_i) / tau
+  // evaluated for the pairs (i, opp(i)), whose eu differ only in sign.
+  const R base = rsub(R(1), usq15);
+  const R wd0 = rmul(weight<R>(0), d), wd1 = rmul(weight<R>(1), d),
+          wd2 = rmul(weight<R>(4), d);
+  f[0] = rfma(rsub(rmul(wd0, base), f[0]), omega, f[0]);
 #pragma unroll
-  for (int i = 0; i < Q; ++i) {
+  for (int i = 1; i <= 9; ++i) {
     R eu = R(0);
     if (ex(i)) eu = ex(i) > 0 ? radd(eu, ux) : rsub(eu, ux);
     if (ey(i)) eu = ey(i) > 0 ? radd(eu, uy) : rsub(eu, uy);
     if (ez(i)) eu = ez(i) > 0 ? radd(eu, uz) : rsub(eu, uz);
-    const R poly = rsub(rfma(rmul(R(4.5), eu), eu, rfma(R(3), eu, R(1))), usq15);
-    const R feq = rmul(rmul(weight<R>(i), d), poly);
-    f[i] = rfma(rsub(feq, f[i]), omega, f[i]);
+    const R sym = rfma(rmul(R(4.5), eu), eu, base);
+    const R anti = rmul(R(3), eu);
+    const R wd = (i <= 3) ? wd1 : wd2;
+    const R feq_i = rmul(wd, radd(sym, anti));
+    const R feq_o = rmul(wd, rsub(sym, anti));
+    f[i] = rfma(rsub(feq_i, f[i]), omega, f[i]);
+    f[opp(i)] = rfma(rsub(feq_o, f[opp(i)]), omega, f[opp(i)]);
   }
 }
 
@@ -191,7 +200,7 @@ static __global__ void k_build_nbr(const uint32_t* __restrict__ mask,
 
 // ---- two-pass kernels -----------------------------------------------------------
 // blockDim (32, 4): a warp covers 32 x-consecutive nodes of one row.
-template <typename T, int PHASE>
+template <typename T, int PHASE, bool WRITE_RHO>
 __global__ void __launch_bounds__(128)
     k_density(const T* __restrict__ pop, const uint32_t* __restrict__ nbw,
               typename Pop<T>::Real* __restrict__ rho,
@@ -215,45 +224,8 @@ __global__ void __launch_bounds__(128)
     gather<T, PHASE>(pop, g.plane, a, nb, n, R(p.rho_shift), f);
     d = sum_density<R>(p, g, s, y, f);
   }
-  rho[n] = d;
-  psi[n] = psi_of<R>(p, d);
-}
-
-template <typename T, int PHASE, bool WRITE_U>
-__global__ void __launch_bounds__(128)
-    k_update(T* __restrict__ pop, const uint32_t* __restrict__ nbw,
-             const typename Pop<T>::Real* __restrict__ rho,
-             const typename Pop<T>::Real* __restrict__ psi,
-             float* __restrict__ vel, Geom g, Phys p, StepArgs s) {
-  using R = typename Pop<T>::Real;
-  const int x = blockIdx.x * 32 + threadIdx.x;
-  const int y = blockIdx.y * blockDim.y + threadIdx.y;
-  const int z = blockIdx.z;
-  if (x >= g.lx || y >= g.ly) return;
-  const int n = (int)node_index(g, x, y, z);
-  const uint32_t nb = nbw[n];
-  if (!(nb & NB_SELF)) return;
-  const R shift = R(p.rho_shift);
-  Nbr a;
-  a.init(g, x, y, z);
-  R f[Q];
-  R ux = R(0), uy = R(0), uz = R(0);
-  if (nb_kind(nb)) {
-    slab_populations<R>(R(slab_density(p, nb_kind(nb))), f);
-  } else {
-    gather<T, PHASE>(pop, g.plane, a, nb, n, shift, f);
-    const R d = rho[n];
-    collide<R>(
-        p, d, psi[n],
-        [&](int i) { return __ldg(psi + a.idx(ex(i), ey(i), ez(i))); }, f,
-        ux, uy, uz);
-  }
-  if (WRITE_U) {
-    vel[3 * (long long)n] = (float)ux;
-    vel[3 * (long long)n + 1] = (float)uy;
-    vel[3 * (long long)n + 2] = (float)uz;
-  }
-  scatter<T, PHASE>(pop, g.plane, a, nb, n, shift, f);
+  if (WRITE_RHO) rho[n] = d;
+  store_psi<R>(psi, g, x, y, z, psi_of<R>(p, d));
 }
 
 // ---- initialisation (multiphaselbm_init, include/iteration_kernel.cuh:9-29) --
@@ -278,7 +250,7 @@ __global__ void k_init(T* __restrict__ pop, const uint32_t* __restrict__ mask,
     Pop<T>::st(pop + i * g.plane + n, weight<R>(i) * r0, shift * weight<R>(i));
   const R r = fluid_at(mask, g, x, y, z) ? r0 : R(p.rhos);
   rho[n] = r;
-  psi[n] = psi_of<R>(p, r);
+  store_psi<R>(psi, g, x, y, z, psi_of<R>(p, r));
 }
 
 }  // namespace mlbm

@@ -8,6 +8,7 @@
 #pragma once
 
 #include <cuda_fp16.h>
+#include <limits.h>
 #include <stdint.h>
 
 namespace mlbm {
@@ -53,7 +54,43 @@ struct Geom {
   int px;        // row pitch in nodes (multiple of 32)
   int wpr;       // mask words per row = px / 32
   long long plane;  // nodes per population plane = lz * ly * px
+  int pxg;       // psi row pitch (px + 8, see psi_index)
 };
+
+// psi is stored with one ghost layer on every side, so a tile plus its halo
+// is one rectangular box of memory even at the periodic boundaries:
+// psi(x, y, z) at ((z + 1) * (ly + 2) + y + 1) * pxg + x + 4 for x in
+// [-1, lx], y in [-1, ly], z in [-1, lz].  x starts at column 4 so that every
+// 32-aligned tile's halo box starts 16-byte aligned (a TMA requirement).
+__host__ __device__ __forceinline__ long long psi_index(const Geom& g, int x,
+                                                       int y, int z) {
+  return ((long long)(z + 1) * (g.ly + 2) + (y + 1)) * g.pxg + x + 4;
+}
+__host__ __device__ __forceinline__ long long psi_elems(const Geom& g) {
+  return (long long)(g.lz + 2) * (g.ly + 2) * g.pxg;
+}
+
+// Store psi of node (x, y, z) and its periodic ghost copies.
+template <typename R>
+__device__ __forceinline__ void store_psi(R* __restrict__ psi, const Geom& g,
+                                          int x, int y, int z, R v) {
+  const int xs[3] = {x, x == 0 ? g.lx : INT_MIN, x == g.lx - 1 ? -1 : INT_MIN};
+  const int ys[3] = {y, y == 0 ? g.ly : INT_MIN, y == g.ly - 1 ? -1 : INT_MIN};
+  const int zs[3] = {z, z == 0 ? g.lz : INT_MIN, z == g.lz - 1 ? -1 : INT_MIN};
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    if (zs[c] == INT_MIN) continue;
+#pragma unroll
+    for (int b = 0; b < 3; ++b) {
+      if (ys[b] == INT_MIN) continue;
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        if (xs[a] == INT_MIN) continue;
+        psi[psi_index(g, xs[a], ys[b], zs[c])] = v;
+      }
+    }
+  }
+}
 
 __device__ __forceinline__ long long node_index(const Geom& g, int x, int y,
                                                 int z) {
@@ -115,6 +152,7 @@ struct Phys {
   int inlet_width, outlet_width;
   float rho_inlet, rho_outlet;
   float rho_shift;  // FP16 storage shift (rho0)
+  float omega;      // 1/tau rounded once, as the reference's inv_tau
 };
 
 // Per-launch step arguments of the reference's multiphaselbm_iteration
@@ -137,6 +175,9 @@ __device__ __forceinline__ double radd(double a, double b) { return __dadd_rn(a,
 __device__ __forceinline__ double rsub(double a, double b) { return __dsub_rn(a, b); }
 __device__ __forceinline__ double rfma(double a, double b, double c) { return __fma_rn(a, b, c); }
 __device__ __forceinline__ double rdiv(double a, double b) { return __ddiv_rn(a, b); }
+// correctly rounded reciprocal: the reference's (float)(1.0 / rho)
+__device__ __forceinline__ float rrcp(float a) { return __frcp_rn(a); }
+__device__ __forceinline__ double rrcp(double a) { return __drcp_rn(a); }
 
 __device__ __forceinline__ float expr(float v) { return expf(v); }
 __device__ __forceinline__ double expr(double v) { return exp(v); }

@@ -132,7 +132,7 @@ __global__ void __launch_bounds__(512)
       if (wP & NB_SELF) {
         const R d = nb_kind(wP) ? R(slab_density(p, nb_kind(wP)))
                                 : sum_density<R>(p, g, a, y, fP);
-        psi[nP] = psi_of<R>(p, d);
+        store_psi<R>(psi, g, x, y, zp, psi_of<R>(p, d));
         if (OUT & OUT_RHO) rho_out[nP] = d;
       }
       __syncthreads();
@@ -172,13 +172,13 @@ __global__ void __launch_bounds__(512)
       const int zz = wrapc(zu + k, g.lz);
       const int slot = (zu + k + 3) % 3;
       R* dst = win + slot * wplane;
-      const R* src = psi + (long long)zz * plane_nodes;
       for (int j = tid; j < wplane; j += blockDim.x) {
         const int jy = j / wx, jx = j - jy * wx;
         const int gy = wrapc(y0 - 1 + jy, g.ly);
         int gx = x0 - 1 + jx;
         gx = gx < 0 ? gx + g.lx : (gx >= g.lx ? gx - g.lx : gx);
-        dst[j] = (gx >= 0 && gx < g.lx) ? __ldcg(src + gy * g.px + gx) : R(0);
+        dst[j] = (gx >= 0 && gx < g.lx) ? __ldcg(psi + psi_index(g, gx, gy, zz))
+                                        : R(0);
       }
     }
     loaded = 1;
