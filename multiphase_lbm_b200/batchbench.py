@@ -1,0 +1,135 @@
+"""Batching form: many independent porous domains of uneven size.
+
+Workload (defaults): 512 domains; every box edge drawn independently from
+{32, 48, ..., 128}; each domain its own seeded sphere packing (radius
+U[2.5, 7.5], porosity target U[0.35, 0.65]) and wall adhesion G_ads in
+U[-2, 0] (rhos = -ln(1 - G_ads/G), G = -6); the drainage boundaries of the
+200^3 case scaled to the box (inlet slab round(8 lx / 200) >= 1 at rho 0.10,
+outlet plane x = lx - 1 at rho 1.95, pores start at rho 2.0); FP16 storage.
+
+Two executions of the same steps, bit-identical results:
+  * batched -- mlbm_batch_iterate: one persistent density launch and one
+    persistent update launch per step for all domains, CUDA graphs, work-item
+    shape from the autotuner;
+  * plain   -- each domain advanced by its own mlbm_iterate calls, one domain
+    after the other (sequential per-domain launches).
+Both are timed with CUDA events over `--steps` steps (a bounded sample of the
+5,000-step run); solves/s = domains / (time for `--solve-steps` steps),
+extrapolated from the sample at the measured per-step rate.
+
+Run: python -m multiphase_lbm_b200.batchbench [--domains 512 --steps 100]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import sys
+import time
+
+import numpy as np
+
+from . import batch, capi, host
+
+EDGES = list(range(32, 129, 16))
+
+
+def make_domains(n, seed=3):
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(n):
+        shape = tuple(int(v) for v in rng.choice(EDGES, 3))
+        por = float(rng.uniform(0.35, 0.65))
+        gads = float(rng.uniform(-2.0, 0.0))
+        fluid, _ = host.generate_packing(shape, 2.5, 7.5, por, seed * 100003 + i)
+        rhos = -math.log(1.0 - gads / -6.0)
+        params = capi.default_params(
+            G=-6.0, tau=1.0, rhos=rhos, inlet_width=max(1, round(8 * shape[0] / 200)),
+            outlet_width=1, rho_inlet=0.10, rho_outlet=1.95, rho_shift=1.0)
+        out.append((shape, fluid, np.full(shape, 2.0, np.float32), params))
+    return out
+
+
+def run(ndomains=512, steps=100, storage=capi.STORE_F16, solve_steps=5000,
+        seed=3, log=print) -> dict:
+    import torch
+    t0 = time.time()
+    doms = make_domains(ndomains, seed)
+    nodes = sum(int(np.prod(s)) for s, _, _, _ in doms)
+    log(f"{ndomains} domains, {nodes / 1e6:.1f} M nodes, geometry in "
+        f"{time.time() - t0:.1f} s")
+
+    # ---- batched --------------------------------------------------------
+    b = batch.Batch(storage)
+    for shape, fl, rho, p in doms:
+        b.add(fl, rho, p)
+    tuning = b.autotune(2)
+    b.iterate(3)
+    b.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    t_wall = time.perf_counter()
+    e0.record()
+    b.iterate(steps)
+    b.synchronize()
+    e1.record()
+    torch.cuda.synchronize()
+    wall_b = time.perf_counter() - t_wall
+    ms_b = e0.elapsed_time(e1) / steps
+    mem = b.nbytes()
+    b.close()
+
+    # ---- plain sequential per-domain launches ---------------------------
+    lats = []
+    for shape, fl, rho, p in doms:
+        lat = capi.Lattice(shape, storage=storage)
+        lat.set_params(p)
+        lat.upload(fl, rho)
+        lat.initialize()
+        lat.iterate(0, 3)
+        lats.append(lat)
+    torch.cuda.synchronize()
+    t_wall = time.perf_counter()
+    e0.record()
+    for k in range(steps):
+        for lat in lats:
+            lat.iterate(3 + k, 1)
+    e1.record()
+    torch.cuda.synchronize()
+    wall_p = time.perf_counter() - t_wall
+    ms_p = e0.elapsed_time(e1) / steps
+    for lat in lats:
+        lat.close()
+
+    res = {
+        "domains": ndomains, "nodes": nodes, "storage": storage,
+        "sample_steps": steps, "solve_steps": solve_steps,
+        "batched_ms_per_step": round(ms_b, 4),
+        "plain_ms_per_step": round(ms_p, 4),
+        "batched_mlups": round(nodes / ms_b / 1e3, 1),
+        "plain_mlups": round(nodes / ms_p / 1e3, 1),
+        "batched_solves_per_s": round(ndomains / (ms_b * solve_steps / 1e3), 4),
+        "plain_solves_per_s": round(ndomains / (ms_p * solve_steps / 1e3), 4),
+        "speedup": round(ms_p / ms_b, 3),
+        "wall_s": {"batched": round(wall_b, 2), "plain": round(wall_p, 2)},
+        "tuning": tuning, "device_bytes": mem,
+    }
+    return res
+
+
+def main(argv=None) -> int:
+    ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
+    ap.add_argument("--domains", type=int, default=512)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--storage", default="f16", choices=["f16", "f32"])
+    ap.add_argument("--seed", type=int, default=3)
+    a = ap.parse_args(argv)
+    st = capi.STORE_F16 if a.storage == "f16" else capi.STORE_F32
+    res = run(a.domains, a.steps, st, seed=a.seed,
+              log=lambda s: print(s, file=sys.stderr, flush=True))
+    print(json.dumps(res))
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

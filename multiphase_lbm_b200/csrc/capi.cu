@@ -211,6 +211,11 @@ mlbm_status launch_steps(mlbm_lattice* lat, int64_t step0, int32_t nsteps,
   const bool fused = lat->step_kernel == MLBM_KERNEL_FUSED && lat->fused.ok;
   if (lat->step_kernel == MLBM_KERNEL_FUSED && !lat->fused.ok)
     return fail(MLBM_ERR_ARG, "fused kernel does not fit this lattice");
+  if ((flags & MLBM_ITER_WRITE_VELOCITY) && !lat->vel) {
+    // the velocity field is allocated on first request
+    CUDA_TRY(cudaMalloc((void**)&lat->vel, (size_t)lat->g.plane * 3 * sizeof(float)),
+             "velocity allocation");
+  }
   for (int32_t s = 0; s < nsteps; ++s) {
     StepArgs a{(long long)(step0 + s), reverse, inject_type};
     const bool last = s == nsteps - 1;
@@ -363,8 +368,8 @@ uint64_t mlbm_lattice_bytes(int32_t lx, int32_t ly, int32_t lz,
          + (uint64_t)psi_elems(g) * real_bytes(storage)  // psi with ghosts
          + np * 4                             // initial density
          + (uint64_t)g.lz * g.ly * g.wpr * 4  // mask
-         + np * 12                            // velocity
          + np * 4;                            // neighbour words
+  // (the velocity field, 12 bytes per node, is allocated on first request)
 }
 
 mlbm_status mlbm_lattice_create(int32_t lx, int32_t ly, int32_t lz,
@@ -402,7 +407,6 @@ mlbm_status mlbm_lattice_create(int32_t lx, int32_t ly, int32_t lz,
   alloc(&lat->psi, (size_t)psi_elems(lat->g) * real_bytes(storage));
   alloc((void**)&lat->rho_init, np * sizeof(float));
   alloc((void**)&lat->mask, mask_words * sizeof(uint32_t));
-  alloc((void**)&lat->vel, np * 3 * sizeof(float));
   alloc((void**)&lat->nbw, np * sizeof(uint32_t));
   const size_t ncount = (size_t)max_tiles(lat->g);
   alloc((void**)&lat->pdone, ncount * sizeof(unsigned));

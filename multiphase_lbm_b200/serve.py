@@ -1,0 +1,227 @@
+"""Serving form: a request loop with continuous batching.
+
+Each request is one porous domain: box edges drawn from {48, 64, ..., 192},
+a seeded sphere packing (radius U[2.5, 7.5], porosity U[0.35, 0.65]), inlet
+density U[0.05, 0.3], wall adhesion G_ads U[-2, 0], a step budget
+U[2000, 50000] (times --budget-scale), and a tolerance that picks FP32 or
+FP16 storage.  A request is done when its budget is spent or its saturation
+changed by less than 1e-5 over the last 1000 steps.
+
+Batched server: requests arrive as a Poisson stream; the loop admits every
+arrived request whose lattice fits under the HBM cap into the FP32 or FP16
+batch (mlbm_batch_add; the geometry is built on the host while the GPU runs
+the previous chunk), advances both batches by `chunk` steps (their launches
+overlap on the device), and retires finished requests (mlbm_batch_remove),
+freeing memory for the queue.  FIFO baseline: the same requests, in arrival
+order, each run alone on the whole GPU with mlbm_iterate.
+
+Reported: solves/s, p50/p95/p99 time-to-result (arrival to result on the
+host), for both.  Each result (final saturation and density field) is the
+same in the batch as alone: the batched kernels are bit-identical to the
+single-domain ones (tests/test_gpu_batch.py, tests/test_gpu_serve.py).
+
+Run: python -m multiphase_lbm_b200.serve --requests 48 --rate 20
+"""
+from __future__ import annotations
+
+import argparse
+import heapq
+import json
+import math
+import sys
+import time
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import batch, capi, host
+
+EDGES = list(range(48, 193, 16))
+CONVERGENCE_DS = 1e-5
+CONVERGENCE_STEPS = 1000
+
+
+@dataclass
+class Request:
+    rid: int
+    arrival: float
+    shape: tuple
+    seed: int
+    porosity: float
+    rho_in: float
+    g_ads: float
+    budget: int
+    fp16_ok: bool
+    # filled by the server
+    done_at: float = -1.0
+    steps: int = 0
+    saturation: float = float("nan")
+    converged: bool = False
+    history: list = field(default_factory=list)
+
+
+def make_requests(n, rate, seed=7, budget_scale=1.0, edges=EDGES):
+    rng = np.random.default_rng(seed)
+    t = 0.0
+    out = []
+    for i in range(n):
+        t += rng.exponential(1.0 / rate)
+        shape = tuple(int(v) for v in rng.choice(edges, 3))
+        budget = max(CONVERGENCE_STEPS,
+                     int(round(rng.uniform(2000, 50000) * budget_scale)))
+        out.append(Request(i, t, shape, int(rng.integers(1 << 30)),
+                           float(rng.uniform(0.35, 0.65)),
+                           float(rng.uniform(0.05, 0.3)),
+                           float(rng.uniform(-2.0, 0.0)), budget,
+                           bool(rng.random() < 0.5)))
+    return out
+
+
+def geometry(req: Request):
+    fluid, _ = host.generate_packing(req.shape, 2.5, 7.5, req.porosity, req.seed)
+    rho = np.full(req.shape, 2.0, np.float32)
+    rhos = -math.log(1.0 - req.g_ads / -6.0)
+    params = capi.default_params(
+        G=-6.0, tau=1.0, rhos=rhos,
+        inlet_width=max(1, round(8 * req.shape[0] / 200)), outlet_width=1,
+        rho_inlet=req.rho_in, rho_outlet=1.95, rho_shift=1.0)
+    return fluid, rho, params
+
+
+def _finished(req: Request) -> bool:
+    if req.steps >= req.budget:
+        return True
+    h = req.history
+    if len(h) >= 2 and h[-1][0] - h[-2][0] >= CONVERGENCE_STEPS:
+        if abs(h[-1][1] - h[-2][1]) < CONVERGENCE_DS:
+            req.converged = True
+            return True
+    return False
+
+
+def serve_batched(reqs, hbm_cap=150e9, chunk=CONVERGENCE_STEPS, log=None):
+    """Continuous batching; returns (makespan_s, requests)."""
+    batches = {True: batch.Batch(capi.STORE_F16), False: batch.Batch(capi.STORE_F32)}
+    pending = sorted(reqs, key=lambda r: r.arrival)
+    ready = {}       # rid -> geometry built ahead of admission
+    active = {}      # rid -> (req, batch, domain id, bytes)
+    used = 0
+    t0 = time.perf_counter()
+    qi = 0
+    while qi < len(pending) or active:
+        now = time.perf_counter() - t0
+        # admit arrived requests that fit under the cap
+        while qi < len(pending) and pending[qi].arrival <= now:
+            r = pending[qi]
+            storage = capi.STORE_F16 if r.fp16_ok else capi.STORE_F32
+            need = capi.lattice_bytes(r.shape, storage)
+            if used + need > hbm_cap and active:
+                break
+            fl, rho, p = ready.pop(r.rid, None) or geometry(r)
+            did = batches[r.fp16_ok].add(fl, rho, p)
+            active[r.rid] = (r, batches[r.fp16_ok], did, need)
+            used += need
+            qi += 1
+        if not active:
+            if qi < len(pending):
+                time.sleep(max(0.0, pending[qi].arrival - now))
+            continue
+        # advance every batch by one chunk (asynchronous, overlapping)
+        for b in batches.values():
+            if b.count():
+                b.iterate(chunk)
+        # build geometry of the next arrivals while the GPU works
+        for r in pending[qi:qi + 4]:
+            if r.rid not in ready:
+                ready[r.rid] = geometry(r)
+        for b in batches.values():
+            b.synchronize()
+        done = []
+        for rid, (r, b, did, need) in active.items():
+            r.steps += chunk
+            s = b.lattice(did).stats()["saturation"]
+            r.history.append((r.steps, s))
+            if _finished(r):
+                r.saturation = s
+                r.done_at = time.perf_counter() - t0
+                done.append(rid)
+        for rid in done:
+            r, b, did, need = active.pop(rid)
+            b.remove(did)
+            used -= need
+        if log and done:
+            log(f"t={time.perf_counter() - t0:.2f}s active={len(active)} "
+                f"done+={len(done)} queue={len(pending) - qi}")
+    makespan = time.perf_counter() - t0
+    for b in batches.values():
+        b.close()
+    return makespan, reqs
+
+
+def serve_fifo(reqs, chunk=CONVERGENCE_STEPS, log=None):
+    """Requests one at a time in arrival order, each alone on the GPU."""
+    t0 = time.perf_counter()
+    for r in sorted(reqs, key=lambda q: q.arrival):
+        now = time.perf_counter() - t0
+        if r.arrival > now:
+            time.sleep(r.arrival - now)
+        fl, rho, p = geometry(r)
+        lat = capi.Lattice(r.shape, storage=capi.STORE_F16 if r.fp16_ok
+                           else capi.STORE_F32)
+        lat.set_params(p)
+        lat.upload(fl, rho)
+        lat.initialize()
+        while True:
+            lat.iterate(r.steps, chunk)
+            r.steps += chunk
+            s = lat.stats()["saturation"]
+            r.history.append((r.steps, s))
+            if _finished(r):
+                r.saturation = s
+                break
+        r.done_at = time.perf_counter() - t0
+        lat.close()
+    return time.perf_counter() - t0, reqs
+
+
+def summarise(makespan, reqs):
+    ttr = np.array([r.done_at - r.arrival for r in reqs])
+    return {"requests": len(reqs), "makespan_s": round(makespan, 3),
+            "solves_per_s": round(len(reqs) / makespan, 4),
+            "p50_s": round(float(np.percentile(ttr, 50)), 3),
+            "p95_s": round(float(np.percentile(ttr, 95)), 3),
+            "p99_s": round(float(np.percentile(ttr, 99)), 3),
+            "converged": int(sum(r.converged for r in reqs)),
+            "node_steps": int(sum(np.prod(r.shape) * r.steps for r in reqs))}
+
+
+def main(argv=None) -> int:
+    ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
+    ap.add_argument("--requests", type=int, default=48)
+    ap.add_argument("--rate", type=float, default=20.0)
+    ap.add_argument("--budget-scale", type=float, default=0.1)
+    ap.add_argument("--hbm-cap-gb", type=float, default=150.0)
+    ap.add_argument("--seed", type=int, default=7)
+    ap.add_argument("--no-fifo", action="store_true")
+    a = ap.parse_args(argv)
+    log = lambda s: print(s, file=sys.stderr, flush=True)  # noqa: E731
+    reqs = make_requests(a.requests, a.rate, a.seed, a.budget_scale)
+    mk, done = serve_batched(reqs, a.hbm_cap_gb * 1e9, log=log)
+    out = {"config": {"requests": a.requests, "rate_per_s": a.rate,
+                      "budget_scale": a.budget_scale,
+                      "hbm_cap_gb": a.hbm_cap_gb, "seed": a.seed},
+           "batched": summarise(mk, done)}
+    if not a.no_fifo:
+        reqs2 = make_requests(a.requests, a.rate, a.seed, a.budget_scale)
+        mk2, done2 = serve_fifo(reqs2, log=log)
+        out["fifo"] = summarise(mk2, done2)
+        same = [abs(x.saturation - y.saturation) <= 0.0 and x.steps == y.steps
+                for x, y in zip(sorted(done, key=lambda r: r.rid),
+                                sorted(done2, key=lambda r: r.rid))]
+        out["results_identical"] = int(sum(same))
+    print(json.dumps(out))
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

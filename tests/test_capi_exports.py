@@ -5,10 +5,11 @@ import re
 
 import pytest
 
-from multiphase_lbm_b200 import capi, driver, host
+from multiphase_lbm_b200 import batch, capi, driver, host
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-HEADERS = ["mlbm.h", "mlbm_host.h", "mlbm_driver.h", "mlbm_compat.h"]
+HEADERS = ["mlbm.h", "mlbm_host.h", "mlbm_driver.h", "mlbm_compat.h",
+           "mlbm_batch.h"]
 
 
 def _declared(header):
@@ -31,7 +32,8 @@ def test_bindings_cover_the_abi():
     bound = {n for n, _, _ in capi.SIGNATURES}
     bound |= {n for n, _, _ in host.HOST_SIGNATURES}
     bound |= {n for n, _, _ in driver.DRIVER_SIGNATURES}
-    for header in ("mlbm.h", "mlbm_host.h", "mlbm_driver.h"):
+    bound |= {n for n, _, _ in batch.BATCH_SIGNATURES}
+    for header in ("mlbm.h", "mlbm_host.h", "mlbm_driver.h", "mlbm_batch.h"):
         for name in _declared(header):
             assert name in bound, name
 
