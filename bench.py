@@ -40,9 +40,16 @@ sys.path.insert(0, ROOT)
 
 SHAPE = (200, 200, 200)
 RHO_S = 0.182322  # -ln(1 - G_ads/G) for G_ads = -1, G = -6
-PHYS = dict(G=-6.0, tau=1.0, rhos=RHO_S, inlet_width=8, outlet_width=1,
-            rho_inlet=0.10, rho_outlet=1.95, rhol_spinodal=0.2726,
-            rhog_spinodal=0.0484)
+
+
+def phys(n=200):
+    """Drainage parameters of the n^3 case (slab scaled as round(8 n / 200))."""
+    return dict(G=-6.0, tau=1.0, rhos=RHO_S, inlet_width=max(1, round(8 * n / 200)),
+                outlet_width=1, rho_inlet=0.10, rho_outlet=1.95,
+                rhol_spinodal=0.2726, rhog_spinodal=0.0484)
+
+
+PHYS = phys(200)
 BYTES_PER_FLUID = {"f32": 152, "f16": 76, "f64": 304}
 
 
@@ -203,6 +210,9 @@ def main():
     ap.add_argument("--storage", default="f32", choices=["f32", "f16", "f64"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--size", type=int, default=200,
+                    help="lattice edge (profiling runs use a smaller case)")
+    ap.add_argument("--kernel", default="auto", choices=["auto", "fused", "two-pass"])
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -223,15 +233,17 @@ def main():
     from multiphase_lbm_b200 import capi
     storage = {"f32": capi.STORE_F32, "f16": capi.STORE_F16,
                "f64": capi.STORE_F64}[args.storage]
-    fluid, rho, nspheres = workload()
+    fluid, rho, nspheres = workload((args.size,) * 3)
     n_nodes = fluid.size
     n_fluid = int(fluid.sum())
-    params = capi.default_params(**PHYS, rho_shift=1.0)
+    params = capi.default_params(**phys(args.size), rho_shift=1.0)
 
     lat = capi.Lattice(fluid.shape, storage=storage, device=local)
     lat.set_params(params)
     lat.upload(fluid, rho)
     lat.initialize()
+    lat.set_step_kernel({"auto": capi.KERNEL_AUTO, "fused": capi.KERNEL_FUSED,
+                         "two-pass": capi.KERNEL_TWO_PASS}[args.kernel])
     step = 0
     lat.iterate(step, args.warmup)
     step += args.warmup
@@ -273,7 +285,7 @@ def main():
                       args.steps, dist)
 
     cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and args.size == 200:
         cpu = cpu_reference_sample(fluid, rho)
 
     line = {

@@ -185,6 +185,16 @@ mlbm_status mlbm_set_step_kernel(mlbm_lattice* lat, int32_t kind);
  * between a plane's density pass and its update pass (0 = 4, at least 2). */
 mlbm_status mlbm_set_tuning(mlbm_lattice* lat, int32_t rows_per_item,
                             int32_t plane_lag);
+/* Shape of the two-pass update kernel: tile rows (block = 32 x rows
+ * threads, 1..8) and planes walked per block (1..1024).  Default 4 x 16. */
+mlbm_status mlbm_set_update_shape(mlbm_lattice* lat, int32_t rows,
+                                  int32_t planes);
+/* Time candidate update shapes on this lattice and keep the fastest.  The
+ * trial steps are real steps (step0, step0+1, ...): the lattice advances by
+ * *steps_done of them.  out (optional, 2 ints) receives rows, planes. */
+mlbm_status mlbm_autotune(mlbm_lattice* lat, int64_t step0,
+                          int32_t trial_steps, int32_t* out,
+                          int32_t* steps_done);
 /* Wait for the lattice's stream and report a device-side failure (a bounded
  * wait of the fused kernel that ran out: MLBM_ERR_TIMEOUT; the lattice must
  * then be initialised again). */

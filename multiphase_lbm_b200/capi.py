@@ -111,6 +111,8 @@ SIGNATURES = [
     ("mlbm_set_step_kernel", C.c_int, [_VP, C.c_int32]),
     ("mlbm_set_tuning", C.c_int, [_VP, C.c_int32, C.c_int32]),
     ("mlbm_synchronize", C.c_int, [_VP]),
+    ("mlbm_set_update_shape", C.c_int, [_VP, C.c_int32, C.c_int32]),
+    ("mlbm_autotune", C.c_int, [_VP, C.c_int64, C.c_int32, _VP, _VP]),
     ("mlbm_phase_stats_noalloc", C.c_int, [_VP, _VP, C.c_int32, C.c_int32,
                                            C.c_int32, C.POINTER(Params), _VP,
                                            C.POINTER(Stats)]),
@@ -181,6 +183,18 @@ class Lattice:
 
     def set_tuning(self, rows_per_item: int = 0, plane_lag: int = 0) -> None:
         check(lib().mlbm_set_tuning(self.h, rows_per_item, plane_lag))
+
+    def set_update_shape(self, rows: int = 4, planes: int = 16) -> None:
+        check(lib().mlbm_set_update_shape(self.h, rows, planes))
+
+    def autotune(self, step0: int, trial_steps: int = 4):
+        """Pick the update shape by timing; returns (rows, planes, steps the
+        lattice advanced)."""
+        out = np.zeros(2, np.int32)
+        done = C.c_int32()
+        check(lib().mlbm_autotune(self.h, step0, trial_steps, out.ctypes.data,
+                                  C.byref(done)))
+        return int(out[0]), int(out[1]), done.value
 
     def synchronize(self) -> None:
         check(lib().mlbm_synchronize(self.h))

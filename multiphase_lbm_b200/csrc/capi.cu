@@ -727,6 +727,60 @@ mlbm_status mlbm_set_tuning(mlbm_lattice* lat, int32_t rows_per_item,
   return MLBM_OK;
 }
 
+mlbm_status mlbm_set_update_shape(mlbm_lattice* lat, int32_t rows,
+                                  int32_t planes) {
+  if (mlbm_status st = check_lat(lat)) return st;
+  if (rows < 1 || rows > 8 || planes < 1 || planes > 1024)
+    return fail(MLBM_ERR_ARG, "invalid update shape %d x %d", rows, planes);
+  if (mlbm_status st = activate(lat)) return st;
+  CUDA_TRY(cudaStreamSynchronize(lat->stream), "update shape");
+  return setup_update(lat, rows, planes);
+}
+
+mlbm_status mlbm_autotune(mlbm_lattice* lat, int64_t step0,
+                          int32_t trial_steps, int32_t* out,
+                          int32_t* steps_done) {
+  if (mlbm_status st = check_lat(lat)) return st;
+  if (!lat->initialized) return fail(MLBM_ERR_STATE, "autotune before initialize");
+  if (trial_steps < 1) trial_steps = 2;
+  if (mlbm_status st = activate(lat)) return st;
+  const int rows_c[] = {1, 2, 4, 8};
+  const int planes_c[] = {2, 4, 8, 16, 32};
+  cudaEvent_t e0, e1;
+  CUDA_TRY(cudaEventCreate(&e0), "autotune");
+  CUDA_TRY(cudaEventCreate(&e1), "autotune");
+  float best = 1e30f;
+  int br = lat->zm.By, bp = lat->zm.Dz;
+  int64_t step = step0;
+  for (int r : rows_c)
+    for (int pl : planes_c) {
+      if (mlbm_status st = setup_update(lat, r, pl)) return st;
+      if (mlbm_status st = mlbm_iterate(lat, step, 1, 1, 0, 0)) return st;
+      step += 1;
+      cudaEventRecord(e0, lat->stream);
+      if (mlbm_status st = mlbm_iterate(lat, step, trial_steps, 1, 0, 0)) return st;
+      step += trial_steps;
+      cudaEventRecord(e1, lat->stream);
+      CUDA_TRY(cudaEventSynchronize(e1), "autotune");
+      float ms = 0;
+      cudaEventElapsedTime(&ms, e0, e1);
+      if (ms < best) {
+        best = ms;
+        br = r;
+        bp = pl;
+      }
+    }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (mlbm_status st = setup_update(lat, br, bp)) return st;
+  if (out) {
+    out[0] = br;
+    out[1] = bp;
+  }
+  if (steps_done) *steps_done = (int32_t)(step - step0);
+  return MLBM_OK;
+}
+
 mlbm_status mlbm_synchronize(mlbm_lattice* lat) {
   if (mlbm_status st = check_lat(lat)) return st;
   if (mlbm_status st = activate(lat)) return st;

@@ -34,25 +34,32 @@ namespace mlbm {
 constexpr uint32_t NB_SELF = 1u;
 __host__ __device__ constexpr int nb_kind(uint32_t nb) { return (nb >> 19) & 3; }
 
-// Wrapped neighbour offsets of one node: x-1, x, x+1 and the 9 row offsets
-// of (y+dy, z+dz), dy, dz in {-1, 0, 1}.  Node indices fit 32 bits (checked
-// when the lattice is created).
+// Neighbour indices of one node: the index of (x+dx, y+dy, z+dz) is
+// n + dx + dy*px + dz*ly*px (the displacement part is the same for every
+// thread of a launch) plus a per-thread correction for each axis that wraps
+// around the periodic boundary; a D3Q19 direction has at most two nonzero
+// components, so an index costs one or two integer adds.  Node indices fit
+// 32 bits (checked when the lattice is created).
 struct Nbr {
-  int xm, x0, xp;
-  int r[3][3];
+  int n, px, pz;            // own index, row pitch, plane pitch
+  int cxm, cxp, cym, cyp, czm, czp;  // wrap corrections for -1 / +1 moves
   __device__ __forceinline__ void init(const Geom& g, int x, int y, int z) {
-    xm = x == 0 ? g.lx - 1 : x - 1;
-    x0 = x;
-    xp = x == g.lx - 1 ? 0 : x + 1;
-    const int ys[3] = {y == 0 ? g.ly - 1 : y - 1, y, y == g.ly - 1 ? 0 : y + 1};
-    const int zs[3] = {z == 0 ? g.lz - 1 : z - 1, z, z == g.lz - 1 ? 0 : z + 1};
-#pragma unroll
-    for (int a = 0; a < 3; ++a)
-#pragma unroll
-      for (int b = 0; b < 3; ++b) r[a][b] = (zs[b] * g.ly + ys[a]) * g.px;
+    px = g.px;
+    pz = g.ly * g.px;
+    n = z * pz + y * px + x;
+    cxm = x == 0 ? g.lx : 0;
+    cxp = x == g.lx - 1 ? -g.lx : 0;
+    cym = y == 0 ? g.ly * px : 0;
+    cyp = y == g.ly - 1 ? -g.ly * px : 0;
+    czm = z == 0 ? g.lz * pz : 0;
+    czp = z == g.lz - 1 ? -g.lz * pz : 0;
   }
   __device__ __forceinline__ int idx(int dx, int dy, int dz) const {
-    return r[dy + 1][dz + 1] + (dx < 0 ? xm : (dx > 0 ? xp : x0));
+    int v = n + dx + dy * px + dz * pz;
+    if (dx) v += dx < 0 ? cxm : cxp;
+    if (dy) v += dy < 0 ? cym : cyp;
+    if (dz) v += dz < 0 ? czm : czp;
+    return v;
   }
 };
 
@@ -73,7 +80,8 @@ __device__ __forceinline__ void gather(const T* __restrict__ pop,
       src = a.idx(-ex(i), -ey(i), -ez(i));
       slot = opp(i);
     }
-    f[i] = Pop<T>::ld(pop + (long long)slot * plane + src, s);
+    const T* base = pop + (long long)slot * plane;
+    f[i] = Pop<T>::ld(base + src, s);
   }
 }
 
@@ -94,7 +102,8 @@ __device__ __forceinline__ void scatter(T* __restrict__ pop, long long plane,
       dst = a.idx(ex(i), ey(i), ez(i));
       slot = i;
     }
-    Pop<T>::st(pop + (long long)slot * plane + dst, f[i], s);
+    T* base = pop + (long long)slot * plane;
+    Pop<T>::st(base + dst, f[i], s);
   }
 }
 
