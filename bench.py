@@ -68,15 +68,22 @@ def load_peaks():
     return 6650.0, "fallback"
 
 
-def load_traffic(storage):
-    """DRAM bytes per time step from the committed ncu summary, if present."""
+def load_traffic(kernel, storage):
+    """DRAM bytes per time step of `kernel` at 200^3 from the committed ncu
+    summary (profiles/traffic.json), if present."""
     p = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(p):
-        d = json.load(open(p))
+        d = json.load(open(p)).get(kernel, {})
         v = d.get(storage)
         if v is not None:
             return float(v)
     return None
+
+
+# roofline label and launches per step of each step kernel
+KERNEL_INFO = {3: ("compact", "k_compact_step (single pass, compact layout)", 1),
+               2: ("two-pass", "time step (k_density + k_update_zm)", 2),
+               1: ("fused", "k_step_fused (persistent)", 1)}
 
 
 class ClockSampler:
@@ -212,7 +219,8 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--size", type=int, default=200,
                     help="lattice edge (profiling runs use a smaller case)")
-    ap.add_argument("--kernel", default="auto", choices=["auto", "fused", "two-pass"])
+    ap.add_argument("--kernel", default="auto",
+                    choices=["auto", "compact", "fused", "two-pass"])
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -242,8 +250,11 @@ def main():
     lat.set_params(params)
     lat.upload(fluid, rho)
     lat.initialize()
-    lat.set_step_kernel({"auto": capi.KERNEL_AUTO, "fused": capi.KERNEL_FUSED,
-                         "two-pass": capi.KERNEL_TWO_PASS}[args.kernel])
+    kernel_id = {"auto": capi.KERNEL_AUTO, "compact": capi.KERNEL_COMPACT,
+                 "fused": capi.KERNEL_FUSED,
+                 "two-pass": capi.KERNEL_TWO_PASS}[args.kernel]
+    lat.set_step_kernel(kernel_id)
+    kname, klabel, klaunches = KERNEL_INFO[lat.step_kernel]
     step = 0
     lat.iterate(step, args.warmup)
     step += args.warmup
@@ -276,13 +287,13 @@ def main():
     peak, peak_kind = load_peaks()
     alg_bytes = n_fluid * BYTES_PER_FLUID[args.storage] + n_nodes / 8
     achieved = alg_bytes / s_per_step / 1e9
-    traffic = load_traffic(args.storage)
+    traffic = load_traffic(kname, args.storage) if args.size == 200 else None
 
     # ---- end to end through the C ABI with host buffers --------------------
     e2e = None
     if not args.no_e2e:
         e2e = run_e2e(capi, torch, fluid, rho, params, storage, local,
-                      args.steps, dist)
+                      args.steps, dist, kernel_id)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline and args.size == 200:
@@ -308,10 +319,10 @@ def main():
                      "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 4),
                      "traffic": traffic, "peak_kind": peak_kind,
-                     "kernel": "time step (k_density + k_update)",
+                     "kernel": klabel,
                      "alg_bytes_per_step": int(alg_bytes)},
         "clocks": clocks.summary(),
-        "gpu_launches": 2 * args.steps,
+        "gpu_launches": klaunches * args.steps,
     }
     if e2e:
         line["e2e"] = e2e
@@ -325,12 +336,14 @@ def main():
     return 0
 
 
-def run_e2e(capi, torch, fluid, rho, params, storage, device, steps, dist):
+def run_e2e(capi, torch, fluid, rho, params, storage, device, steps, dist,
+            kernel_id=0):
     """MLUPS through the public C ABI with host buffers (pinned)."""
     fl_h = torch.from_numpy(fluid).pin_memory().numpy()
     rho_h = torch.from_numpy(rho).pin_memory().numpy()
     out_h = torch.empty(fluid.shape, dtype=torch.float32).pin_memory().numpy()
     lat = capi.Lattice(fluid.shape, storage=storage, device=device)
+    lat.set_step_kernel(kernel_id)
     lat.set_params(params)
     if dist:
         dist.barrier()

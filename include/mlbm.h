@@ -172,14 +172,34 @@ mlbm_status mlbm_iterate(mlbm_lattice* lat, int64_t step0, int32_t nsteps,
                          int32_t reverse, uint32_t inject_type,
                          uint32_t flags);
 
-/* Which kernels advance the lattice: the two-pass kernels (a density launch
- * and an update launch per step; AUTO, the default) or the fused persistent
- * kernel (one cooperative launch per step, density and update passes
- * interleaved plane by plane).  Both give bit-identical results. */
+/* Which kernels advance the lattice:
+ *   TWO_PASS  a density launch and an update launch per step over the dense
+ *             layout; bit-identical to the reference's kernels;
+ *   FUSED     one cooperative launch per step, the two passes interleaved
+ *             plane by plane; bit-identical to TWO_PASS;
+ *   COMPACT   one launch per step over a fluid-only population layout: the
+ *             populations are read and written once per step and psi of the
+ *             next step is accumulated from the outputs.  FP32 / FP16 storage,
+ *             ly, lz >= 4.  The collision is the same; psi is formed from a
+ *             differently ordered sum of the same populations, so results
+ *             agree with TWO_PASS to rounding (not bit for bit) and are
+ *             deterministic;
+ *   AUTO      (default) COMPACT where supported, else TWO_PASS.
+ * The state moves between the layouts on demand (the dense buffers stay
+ * allocated; COMPACT adds 19 populations and 4 partial sums per fluid node,
+ * allocated on first use). */
 #define MLBM_KERNEL_AUTO 0
 #define MLBM_KERNEL_FUSED 1
 #define MLBM_KERNEL_TWO_PASS 2
+#define MLBM_KERNEL_COMPACT 3
 mlbm_status mlbm_set_step_kernel(mlbm_lattice* lat, int32_t kind);
+/* The kernel the next mlbm_iterate runs (AUTO resolved); -1 for NULL. */
+int32_t mlbm_get_step_kernel(const mlbm_lattice* lat);
+/* Tiling of the COMPACT step: a block walks `rows` full x-rows (y) through
+ * `planes` planes (z); at least two tiles along y and z, each at least two
+ * rows / planes deep.  Default 4 x 8. */
+mlbm_status mlbm_set_compact_shape(mlbm_lattice* lat, int32_t rows,
+                                   int32_t planes);
 /* Tuning of the fused kernel: tile rows (the tile is 32 x rows nodes of an
  * (x, y) plane; 0 = automatic, else 1, 2, 4, 8 or 16) and the lag in planes
  * between a plane's density pass and its update pass (0 = 4, at least 2). */
@@ -189,9 +209,10 @@ mlbm_status mlbm_set_tuning(mlbm_lattice* lat, int32_t rows_per_item,
  * threads, 1..8) and planes walked per block (1..1024).  Default 4 x 16. */
 mlbm_status mlbm_set_update_shape(mlbm_lattice* lat, int32_t rows,
                                   int32_t planes);
-/* Time candidate update shapes on this lattice and keep the fastest.  The
- * trial steps are real steps (step0, step0+1, ...): the lattice advances by
- * *steps_done of them.  out (optional, 2 ints) receives rows, planes. */
+/* Time candidate shapes of the lattice's step kernel (update shape for
+ * TWO_PASS, tiling for COMPACT) and keep the fastest.  The trial steps are
+ * real steps (step0, step0+1, ...): the lattice advances by *steps_done of
+ * them.  out (optional, 2 ints) receives rows, planes. */
 mlbm_status mlbm_autotune(mlbm_lattice* lat, int64_t step0,
                           int32_t trial_steps, int32_t* out,
                           int32_t* steps_done);

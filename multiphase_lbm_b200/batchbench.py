@@ -12,7 +12,11 @@ Two executions of the same steps, bit-identical results:
     persistent update launch per step for all domains, CUDA graphs, work-item
     shape from the autotuner;
   * plain   -- each domain advanced by its own mlbm_iterate calls, one domain
-    after the other (sequential per-domain launches).
+    after the other (sequential per-domain launches), with the same two-pass
+    kernels as the batch.
+A third execution, plain_compact, advances the domains one after the other
+with the compact single-pass step (one launch per step and domain; results
+equal to rounding, not bit for bit).
 Both are timed with CUDA events over `--steps` steps (a bounded sample of the
 5,000-step run); solves/s = domains / (time for `--solve-steps` steps),
 extrapolated from the sample at the measured per-step rate.
@@ -51,7 +55,7 @@ def make_domains(n, seed=3):
 
 
 def run(ndomains=512, steps=100, storage=capi.STORE_F16, solve_steps=5000,
-        seed=3, log=print) -> dict:
+        seed=3, log=print, compact=True) -> dict:
     import torch
     t0 = time.time()
     doms = make_domains(ndomains, seed)
@@ -80,26 +84,32 @@ def run(ndomains=512, steps=100, storage=capi.STORE_F16, solve_steps=5000,
     b.close()
 
     # ---- plain sequential per-domain launches ---------------------------
-    lats = []
-    for shape, fl, rho, p in doms:
-        lat = capi.Lattice(shape, storage=storage)
-        lat.set_params(p)
-        lat.upload(fl, rho)
-        lat.initialize()
-        lat.iterate(0, 3)
-        lats.append(lat)
-    torch.cuda.synchronize()
-    t_wall = time.perf_counter()
-    e0.record()
-    for k in range(steps):
+    def plain(kernel):
+        lats = []
+        for shape, fl, rho, p in doms:
+            lat = capi.Lattice(shape, storage=storage)
+            lat.set_step_kernel(kernel)
+            lat.set_params(p)
+            lat.upload(fl, rho)
+            lat.initialize()
+            lat.iterate(0, 3)
+            lats.append(lat)
+        torch.cuda.synchronize()
+        t_wall = time.perf_counter()
+        e0.record()
+        for k in range(steps):
+            for lat in lats:
+                lat.iterate(3 + k, 1)
+        e1.record()
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - t_wall
+        ms = e0.elapsed_time(e1) / steps
         for lat in lats:
-            lat.iterate(3 + k, 1)
-    e1.record()
-    torch.cuda.synchronize()
-    wall_p = time.perf_counter() - t_wall
-    ms_p = e0.elapsed_time(e1) / steps
-    for lat in lats:
-        lat.close()
+            lat.close()
+        return ms, wall
+
+    ms_p, wall_p = plain(capi.KERNEL_TWO_PASS)
+    ms_c, wall_c = plain(capi.KERNEL_COMPACT) if compact else (None, None)
 
     res = {
         "domains": ndomains, "nodes": nodes, "storage": storage,
@@ -112,6 +122,8 @@ def run(ndomains=512, steps=100, storage=capi.STORE_F16, solve_steps=5000,
         "plain_solves_per_s": round(ndomains / (ms_p * solve_steps / 1e3), 4),
         "speedup": round(ms_p / ms_b, 3),
         "wall_s": {"batched": round(wall_b, 2), "plain": round(wall_p, 2)},
+        "plain_compact_ms_per_step": None if ms_c is None else round(ms_c, 4),
+        "speedup_vs_plain_compact": None if ms_c is None else round(ms_c / ms_b, 3),
         "tuning": tuning, "device_bytes": mem,
     }
     return res

@@ -20,7 +20,7 @@ FIELD_RHO, FIELD_PRESSURE, FIELD_PSI, FIELD_VELOCITY, FIELD_POPULATIONS, \
     FIELD_FLUID = range(6)
 DTYPE_F32, DTYPE_F64, DTYPE_U8 = 0, 1, 2
 ITER_WRITE_VELOCITY = 1
-KERNEL_AUTO, KERNEL_FUSED, KERNEL_TWO_PASS = 0, 1, 2
+KERNEL_AUTO, KERNEL_FUSED, KERNEL_TWO_PASS, KERNEL_COMPACT = 0, 1, 2, 3
 Q = 19
 
 STATUS = {0: "MLBM_OK", 1: "MLBM_ERR_ARG", 2: "MLBM_ERR_CUDA",
@@ -112,6 +112,8 @@ SIGNATURES = [
     ("mlbm_set_tuning", C.c_int, [_VP, C.c_int32, C.c_int32]),
     ("mlbm_synchronize", C.c_int, [_VP]),
     ("mlbm_set_update_shape", C.c_int, [_VP, C.c_int32, C.c_int32]),
+    ("mlbm_set_compact_shape", C.c_int, [_VP, C.c_int32, C.c_int32]),
+    ("mlbm_get_step_kernel", C.c_int32, [_VP]),
     ("mlbm_autotune", C.c_int, [_VP, C.c_int64, C.c_int32, _VP, _VP]),
     ("mlbm_phase_stats_noalloc", C.c_int, [_VP, _VP, C.c_int32, C.c_int32,
                                            C.c_int32, C.POINTER(Params), _VP,
@@ -187,9 +189,19 @@ class Lattice:
     def set_update_shape(self, rows: int = 4, planes: int = 16) -> None:
         check(lib().mlbm_set_update_shape(self.h, rows, planes))
 
+    @property
+    def step_kernel(self) -> int:
+        """The kernel the next iterate runs (KERNEL_COMPACT, ... ; AUTO
+        resolved)."""
+        return int(lib().mlbm_get_step_kernel(self.h))
+
+    def set_compact_shape(self, rows: int = 4, planes: int = 8) -> None:
+        """Tiling of the compact step (rows along y, planes along z)."""
+        check(lib().mlbm_set_compact_shape(self.h, rows, planes))
+
     def autotune(self, step0: int, trial_steps: int = 4):
-        """Pick the update shape by timing; returns (rows, planes, steps the
-        lattice advanced)."""
+        """Pick the shape of the lattice's step kernel by timing; returns
+        (rows, planes, steps the lattice advanced)."""
         out = np.zeros(2, np.int32)
         done = C.c_int32()
         check(lib().mlbm_autotune(self.h, step0, trial_steps, out.ctypes.data,

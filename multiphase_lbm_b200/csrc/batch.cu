@@ -258,7 +258,9 @@ mlbm_status mlbm_batch_add(mlbm_batch* b, int32_t nx, int32_t ny, int32_t nz,
   mlbm_lattice* lat = nullptr;
   if (mlbm_status st = mlbm_lattice_create(nx, ny, nz, b->storage, b->device, &lat))
     return st;
+  // the batch kernels advance the dense layout: keep the domain on it
   mlbm_status st = mlbm_set_stream(lat, b->stream);
+  if (!st) st = mlbm_set_step_kernel(lat, MLBM_KERNEL_TWO_PASS);
   if (!st) st = mlbm_set_params(lat, params);
   if (!st) st = mlbm_upload_fluid_mask(lat, is_fluid);
   if (!st) st = mlbm_upload_rho(lat, rho);

@@ -5,6 +5,7 @@
 // returned as mlbm_status with a message kept per host thread; nothing here
 // exits or falls back to the CPU.
 #include <cuda_runtime.h>
+#include <type_traits>
 
 #include <cstdarg>
 #include <cstdio>
@@ -204,27 +205,47 @@ mlbm_status launch_two_pass(mlbm_lattice* lat, const StepArgs& a, bool wu,
 // One lattice step per launch (two launches for the two-pass kernels, which
 // AUTO selects).  rho is written on the last step of each mlbm_iterate call
 // (the field the caller can read afterwards).
+// The step kernel a lattice runs: AUTO is the compact single-pass step where
+// it supports the lattice (FP32 / FP16 storage), else the two-pass step.
+int effective_kernel(const mlbm_lattice* lat) {
+  if (lat->step_kernel != MLBM_KERNEL_AUTO) return lat->step_kernel;
+  return lat->compact.supported ? MLBM_KERNEL_COMPACT : MLBM_KERNEL_TWO_PASS;
+}
+
 template <typename T>
 mlbm_status launch_steps(mlbm_lattice* lat, int64_t step0, int32_t nsteps,
                          int32_t reverse, uint32_t inject_type,
                          uint32_t flags) {
-  const bool fused = lat->step_kernel == MLBM_KERNEL_FUSED && lat->fused.ok;
-  if (lat->step_kernel == MLBM_KERNEL_FUSED && !lat->fused.ok)
+  const int kind = effective_kernel(lat);
+  const bool fused = kind == MLBM_KERNEL_FUSED && lat->fused.ok;
+  if (kind == MLBM_KERNEL_FUSED && !lat->fused.ok)
     return fail(MLBM_ERR_ARG, "fused kernel does not fit this lattice");
+  bool compact = false;
+  if constexpr (!std::is_same<T, double>::value) compact = kind == MLBM_KERNEL_COMPACT;
   if ((flags & MLBM_ITER_WRITE_VELOCITY) && !lat->vel) {
     // the velocity field is allocated on first request
     CUDA_TRY(cudaMalloc((void**)&lat->vel, (size_t)lat->g.plane * 3 * sizeof(float)),
              "velocity allocation");
   }
+  if (compact) {
+    if (mlbm_status st = compact_enter(lat)) return st;
+  } else {
+    if (mlbm_status st = compact_leave(lat)) return st;
+  }
   for (int32_t s = 0; s < nsteps; ++s) {
     StepArgs a{(long long)(step0 + s), reverse, inject_type};
     const bool last = s == nsteps - 1;
     const bool wu = (flags & MLBM_ITER_WRITE_VELOCITY) && last;
+    const int out = wu ? (OUT_RHO | OUT_VEL) : (last ? OUT_RHO : OUT_NONE);
     mlbm_status st;
-    if (fused)
-      st = launch_fused<T>(lat, a, wu ? (OUT_RHO | OUT_VEL) : (last ? OUT_RHO : OUT_NONE));
-    else
-      st = launch_two_pass<T>(lat, a, wu, last);
+    if constexpr (!std::is_same<T, double>::value) {
+      if (compact) st = launch_compact<T>(lat, a, out);
+      else if (fused) st = launch_fused<T>(lat, a, out);
+      else st = launch_two_pass<T>(lat, a, wu, last);
+    } else {
+      if (fused) st = launch_fused<T>(lat, a, out);
+      else st = launch_two_pass<T>(lat, a, wu, last);
+    }
     if (st) return st;
     lat->phase ^= 1;
     if (wu) lat->vel_valid = true;
@@ -278,6 +299,7 @@ mlbm_status field_out(mlbm_lattice* lat, int32_t field, O* dev_out) {
           lat->vel, dev_out, lat->g);
       break;
     case MLBM_FIELD_POPULATIONS:
+      if (mlbm_status st = compact_sync_dense(lat)) return st;
       if (lat->storage == MLBM_STORE_F32)
         launch_pop_out<float, O>(lat, dev_out);
       else if (lat->storage == MLBM_STORE_F16)
@@ -396,6 +418,7 @@ mlbm_status mlbm_lattice_create(int32_t lx, int32_t ly, int32_t lz,
   lat->storage = storage;
   lat->g = make_geom(lx, ly, lz);
   lat->fused = fused_shape(lat->g, storage, 0, 0);
+  lat->compact.supported = compact_supported(lx, ly, lz, storage);
   const size_t np = (size_t)lat->g.plane;
   const size_t mask_words = (size_t)lz * ly * lat->g.wpr;
   cudaError_t e = cudaSuccess;
@@ -445,6 +468,7 @@ mlbm_status mlbm_lattice_destroy(mlbm_lattice* lat) {
   cudaFree(lat->stats_scratch);
   cudaFree(lat->pdone);
   cudaFree(lat->err);
+  compact_free(lat);
   delete lat;
   return MLBM_OK;
 }
@@ -482,6 +506,7 @@ static mlbm_status upload_mask_impl(mlbm_lattice* lat, const uint8_t* src,
       static_cast<const uint8_t*>(lat->staging), lat->mask, g);
   CUDA_TRY(cudaGetLastError(), "mask pack launch");
   CUDA_TRY(cudaStreamSynchronize(lat->stream), "mask upload");
+  compact_invalidate(lat);
   lat->has_mask = true;
   lat->initialized = false;
   return MLBM_OK;
@@ -542,6 +567,7 @@ mlbm_status mlbm_initialize(mlbm_lattice* lat) {
     default: st = launch_init<double>(lat); break;
   }
   if (st) return st;
+  lat->compact.active = false;  // the initial state is written densely
   lat->phase = 0;
   lat->initialized = true;
   lat->vel_valid = false;
@@ -703,10 +729,14 @@ mlbm_status mlbm_plane_profile(mlbm_lattice* lat, int64_t* n_fluid_x,
 
 mlbm_status mlbm_set_step_kernel(mlbm_lattice* lat, int32_t kind) {
   if (mlbm_status st = check_lat(lat)) return st;
-  if (kind < MLBM_KERNEL_AUTO || kind > MLBM_KERNEL_TWO_PASS)
+  if (kind < MLBM_KERNEL_AUTO || kind > MLBM_KERNEL_COMPACT)
     return fail(MLBM_ERR_ARG, "invalid step kernel %d", kind);
   if (kind == MLBM_KERNEL_FUSED && !lat->fused.ok)
     return fail(MLBM_ERR_ARG, "fused kernel does not fit this lattice");
+  if (kind == MLBM_KERNEL_COMPACT && !lat->compact.supported)
+    return fail(MLBM_ERR_ARG,
+                "compact step needs FP32 or FP16 storage, ly and lz >= 4 and "
+                "a row that fits shared memory");
   lat->step_kernel = kind;
   return MLBM_OK;
 }
@@ -737,6 +767,20 @@ mlbm_status mlbm_set_update_shape(mlbm_lattice* lat, int32_t rows,
   return setup_update(lat, rows, planes);
 }
 
+int32_t mlbm_get_step_kernel(const mlbm_lattice* lat) {
+  return lat ? effective_kernel(lat) : -1;
+}
+
+mlbm_status mlbm_set_compact_shape(mlbm_lattice* lat, int32_t rows,
+                                   int32_t planes) {
+  if (mlbm_status st = check_lat(lat)) return st;
+  if (rows < 2 || rows > 64 || planes < 2 || planes > 4096)
+    return fail(MLBM_ERR_ARG, "invalid compact shape %d x %d", rows, planes);
+  if (mlbm_status st = activate(lat)) return st;
+  CUDA_TRY(cudaStreamSynchronize(lat->stream), "compact shape");
+  return compact_set_shape(lat, rows, planes);
+}
+
 mlbm_status mlbm_autotune(mlbm_lattice* lat, int64_t step0,
                           int32_t trial_steps, int32_t* out,
                           int32_t* steps_done) {
@@ -744,17 +788,33 @@ mlbm_status mlbm_autotune(mlbm_lattice* lat, int64_t step0,
   if (!lat->initialized) return fail(MLBM_ERR_STATE, "autotune before initialize");
   if (trial_steps < 1) trial_steps = 2;
   if (mlbm_status st = activate(lat)) return st;
-  const int rows_c[] = {1, 2, 4, 8};
-  const int planes_c[] = {2, 4, 8, 16, 32};
+  const bool compact = effective_kernel(lat) == MLBM_KERNEL_COMPACT;
+  const int rows_u[] = {1, 2, 4, 8};
+  const int planes_u[] = {2, 4, 8, 16, 32};
+  const int rows_k[] = {2, 3, 4, 6, 8};
+  const int planes_k[] = {4, 8, 16, 32};
+  const int* rows_c = compact ? rows_k : rows_u;
+  const int* planes_c = compact ? planes_k : planes_u;
+  const int nr = compact ? 5 : 4, np = compact ? 4 : 5;
   cudaEvent_t e0, e1;
   CUDA_TRY(cudaEventCreate(&e0), "autotune");
   CUDA_TRY(cudaEventCreate(&e1), "autotune");
   float best = 1e30f;
-  int br = lat->zm.By, bp = lat->zm.Dz;
+  int br = compact ? lat->compact.rows : lat->zm.By;
+  int bp = compact ? lat->compact.planes : lat->zm.Dz;
+  auto apply = [&](int r, int pl) -> mlbm_status {
+    if (compact) {
+      CUDA_TRY(cudaStreamSynchronize(lat->stream), "autotune");
+      return compact_set_shape(lat, r, pl);
+    }
+    return setup_update(lat, r, pl);
+  };
   int64_t step = step0;
-  for (int r : rows_c)
-    for (int pl : planes_c) {
-      if (mlbm_status st = setup_update(lat, r, pl)) return st;
+  for (int ri = 0; ri < nr; ++ri)
+    for (int pi = 0; pi < np; ++pi) {
+      const int r = rows_c[ri], pl = planes_c[pi];
+      if (compact && (lat->g.ly < 2 * r || lat->g.lz < 2 * pl)) continue;
+      if (apply(r, pl) != MLBM_OK) continue;
       if (mlbm_status st = mlbm_iterate(lat, step, 1, 1, 0, 0)) return st;
       step += 1;
       cudaEventRecord(e0, lat->stream);
@@ -772,7 +832,7 @@ mlbm_status mlbm_autotune(mlbm_lattice* lat, int64_t step0,
     }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
-  if (mlbm_status st = setup_update(lat, br, bp)) return st;
+  if (mlbm_status st = apply(br, bp)) return st;
   if (out) {
     out[0] = br;
     out[1] = bp;

@@ -17,6 +17,24 @@ struct FusedShape {
   bool ok;      // false: the fused kernel cannot run this lattice
   bool chosen;  // tile shape fixed (by tuning or at the first launch)
 };
+
+// Fluid-only population layout and tiling of the single-pass step
+// (compact.cuh).  Built from the mask on first use; the dense buffers stay
+// allocated, and the state moves between the two layouts on demand.
+struct CompactState {
+  bool supported = false;  // storage and lattice shape allow the step
+  bool built = false;      // tables match the current mask
+  bool active = false;     // the compact buffer holds the current state
+  long long nfluid = 0, cs = 0;
+  void* cpop = nullptr;        // [Q][cs] populations (T)
+  float* part = nullptr;       // [2][4][cs] part sums of rho (two sets)
+  uint32_t* wbase = nullptr;   // [rows * wpr + 1]
+  int* tabs = nullptr;         // ytab[ly], ztab[lz], ystart[nty+1], zstart[nzc+1]
+  long long cap = 0;           // cs the buffers were allocated for
+  int rows = 4, planes = 8;    // requested tile height and chunk depth
+  int nty = 0, nzc = 0, rows_max = 0;
+  size_t smem = 0;
+};
 }  // namespace mlbm
 
 struct mlbm_lattice {
@@ -50,6 +68,7 @@ struct mlbm_lattice {
   unsigned* pdone = nullptr;               // per-tile progress counters
   int* err = nullptr;                      // device error flag (wait timeout)
   int step_kernel = 0;                     // MLBM_KERNEL_*
+  mlbm::CompactState compact{};            // single-pass step (compact.cuh)
 
   int phase = 0;  // 0: post-collision at opp slots of own node; 1: pushed
   bool has_params = false, has_mask = false, has_rho = false;
@@ -69,4 +88,14 @@ mlbm_status setup_update(mlbm_lattice* lat, int rows, int planes);
 struct StepArgs;
 template <typename T>
 mlbm_status launch_fused(mlbm_lattice* lat, const StepArgs& a, int out);
+// Single-pass step over the compact layout (compact.cu).
+bool compact_supported(int lx, int ly, int lz, int storage);
+mlbm_status compact_set_shape(mlbm_lattice* lat, int rows, int planes);
+mlbm_status compact_enter(mlbm_lattice* lat);   // dense -> compact state
+mlbm_status compact_leave(mlbm_lattice* lat);   // compact -> dense state
+mlbm_status compact_sync_dense(mlbm_lattice* lat);  // dense copy, stay compact
+void compact_invalidate(mlbm_lattice* lat);     // the mask changed
+void compact_free(mlbm_lattice* lat);
+template <typename T>
+mlbm_status launch_compact(mlbm_lattice* lat, const StepArgs& a, int out);
 }  // namespace mlbm

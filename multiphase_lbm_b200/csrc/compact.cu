@@ -1,0 +1,323 @@
+// compact.cu -- host side of the single-pass step over the compact layout
+// (compact.cuh): tables built from the mask, tiling, layout changes, launch.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <mutex>
+#include <vector>
+
+#include "capi_internal.h"
+#include "compact.cuh"
+
+namespace mlbm {
+
+namespace {
+
+dim3 node_block() { return dim3(32, 4, 1); }
+dim3 node_grid(const Geom& g) { return dim3(g.px / 32, (g.ly + 3) / 4, g.lz); }
+
+constexpr int kThreads = 256;
+constexpr size_t kSmemMax = 227 * 1024;
+
+// Part buffers: two sets of [4][cs]; a step from AA phase `ph` reads set ph
+// and writes set ph ^ 1 (the phase alternates with every step).
+CArgs args_of(const mlbm_lattice* lat) {
+  const CompactState& c = lat->compact;
+  const Geom& g = lat->g;
+  const int ph = lat->phase;
+  CArgs a;
+  a.mask = lat->mask;
+  a.wbase = c.wbase;
+  a.ytab = c.tabs;
+  a.ztab = c.tabs + g.ly;
+  a.ystart = c.tabs + g.ly + g.lz;
+  a.zstart = c.tabs + g.ly + g.lz + (c.nty + 1);
+  a.part_rd = c.part + (size_t)ph * 4 * c.cs;
+  a.part_wr = c.part + (size_t)(ph ^ 1) * 4 * c.cs;
+  a.cs = c.cs;
+  a.nty = c.nty;
+  a.nzc = c.nzc;
+  a.rows_max = c.rows_max;
+  return a;
+}
+
+// Split n into k nearly equal parts (each at least 2 when n >= 2k).
+std::vector<int> split(int n, int k) {
+  std::vector<int> s(k + 1);
+  for (int i = 0; i <= k; ++i) s[i] = (int)((long long)i * n / k);
+  return s;
+}
+
+// Tiles of `rows` rows along y and chunks of `planes` planes along z; at
+// least two of each, each at least two rows / planes.
+mlbm_status build_tiling(mlbm_lattice* lat) {
+  CompactState& c = lat->compact;
+  const Geom& g = lat->g;
+  const int nty = std::max(2, std::min(g.ly / 2, g.ly / std::max(1, c.rows)));
+  const int nzc = std::max(2, std::min(g.lz / 2, g.lz / std::max(1, c.planes)));
+  const std::vector<int> ys = split(g.ly, nty), zs = split(g.lz, nzc);
+  int rows_max = 0;
+  for (int t = 0; t < nty; ++t) rows_max = std::max(rows_max, ys[t + 1] - ys[t]);
+  const size_t smem = compact_smem_bytes(rows_max, g.lx, g.wpr);
+  if (smem > kSmemMax)
+    return set_error(MLBM_ERR_ARG, "compact step: tile does not fit shared memory");
+  std::vector<int> tab(g.ly + g.lz + nty + 1 + nzc + 1);
+  for (int t = 0; t < nty; ++t)
+    for (int y = ys[t]; y < ys[t + 1]; ++y)
+      tab[y] = t | (y == ys[t] ? kEdgeLo : 0) | (y == ys[t + 1] - 1 ? kEdgeHi : 0);
+  for (int t = 0; t < nzc; ++t)
+    for (int z = zs[t]; z < zs[t + 1]; ++z)
+      tab[g.ly + z] =
+          t | (z == zs[t] ? kEdgeLo : 0) | (z == zs[t + 1] - 1 ? kEdgeHi : 0);
+  std::copy(ys.begin(), ys.end(), tab.begin() + g.ly + g.lz);
+  std::copy(zs.begin(), zs.end(), tab.begin() + g.ly + g.lz + nty + 1);
+  if (c.tabs) cudaFree(c.tabs);
+  c.tabs = nullptr;
+  cudaError_t e = cudaMalloc((void**)&c.tabs, tab.size() * sizeof(int));
+  if (e == cudaSuccess)
+    e = cudaMemcpy(c.tabs, tab.data(), tab.size() * sizeof(int),
+                   cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) return cuda_fail(e, "compact tiling tables");
+  c.nty = nty;
+  c.nzc = nzc;
+  c.rows_max = rows_max;
+  c.smem = smem;
+  return MLBM_OK;
+}
+
+// Fluid counts per mask word, scanned into wbase; buffers for the fluid
+// nodes.
+mlbm_status build_tables(mlbm_lattice* lat) {
+  CompactState& c = lat->compact;
+  const Geom& g = lat->g;
+  const long long nwords = (long long)g.lz * g.ly * g.wpr;
+  cudaError_t e = cudaStreamSynchronize(lat->stream);
+  if (e != cudaSuccess) return cuda_fail(e, "compact tables");
+  if (c.wbase) cudaFree(c.wbase);
+  c.wbase = nullptr;
+  e = cudaMalloc((void**)&c.wbase, (nwords + 1) * sizeof(uint32_t));
+  if (e != cudaSuccess) return cuda_fail(e, "compact tables");
+  k_word_counts<<<(unsigned)((nwords + 255) / 256), 256, 0, lat->stream>>>(
+      lat->mask, c.wbase, nwords);
+  std::vector<uint32_t> h(nwords + 1);
+  e = cudaMemcpyAsync(h.data(), c.wbase, nwords * sizeof(uint32_t),
+                      cudaMemcpyDeviceToHost, lat->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(lat->stream);
+  if (e != cudaSuccess) return cuda_fail(e, "compact tables");
+  unsigned long long run = 0;
+  for (long long i = 0; i < nwords; ++i) {
+    const uint32_t v = h[i];
+    h[i] = (uint32_t)run;
+    run += v;
+  }
+  h[nwords] = (uint32_t)run;
+  if (run >= (1ull << 31))
+    return set_error(MLBM_ERR_ARG, "compact step: more than 2^31 fluid nodes");
+  e = cudaMemcpy(c.wbase, h.data(), (nwords + 1) * sizeof(uint32_t),
+                 cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) return cuda_fail(e, "compact tables");
+  c.nfluid = (long long)run;
+  c.cs = std::max(64LL, (c.nfluid + 63) / 64 * 64);
+  if (c.cs > c.cap) {
+    cudaFree(c.cpop);
+    cudaFree(c.part);
+    c.cpop = nullptr;
+    c.part = nullptr;
+    c.cap = 0;
+    e = cudaMalloc(&c.cpop, (size_t)c.cs * Q * pop_elem_bytes(lat->storage));
+    if (e == cudaSuccess) e = cudaMalloc((void**)&c.part, (size_t)c.cs * 8 * sizeof(float));
+    if (e != cudaSuccess) {
+      cudaFree(c.cpop);
+      c.cpop = nullptr;
+      cudaGetLastError();
+      return cuda_fail(e, "compact buffers");
+    }
+    c.cap = c.cs;
+  }
+  if (mlbm_status st = build_tiling(lat)) return st;
+  c.built = true;
+  return MLBM_OK;
+}
+
+template <typename T>
+mlbm_status enter_t(mlbm_lattice* lat) {
+  CompactState& c = lat->compact;
+  // the seed goes to the set the next step reads (set `phase`)
+  CArgs a = args_of(lat);
+  float* seed = c.part + (size_t)lat->phase * 4 * c.cs;
+  a.part_wr = seed;
+  k_convert<T, true><<<node_grid(lat->g), node_block(), 0, lat->stream>>>(
+      static_cast<T*>(lat->pop), static_cast<T*>(c.cpop), a, lat->g);
+  cudaError_t e = cudaMemsetAsync(seed + c.cs, 0, 3 * c.cs * sizeof(float), lat->stream);
+  if (e != cudaSuccess) return cuda_fail(e, "compact parts");
+  if (lat->phase == 0)
+    k_seed_parts<T, 0><<<node_grid(lat->g), node_block(), 0, lat->stream>>>(
+        static_cast<const T*>(lat->pop), lat->nbw, a, lat->g, lat->phys);
+  else
+    k_seed_parts<T, 1><<<node_grid(lat->g), node_block(), 0, lat->stream>>>(
+        static_cast<const T*>(lat->pop), lat->nbw, a, lat->g, lat->phys);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(e, "compact entry launch");
+  return MLBM_OK;
+}
+
+template <typename T>
+mlbm_status to_dense_t(mlbm_lattice* lat) {
+  const CArgs a = args_of(lat);
+  k_convert<T, false><<<node_grid(lat->g), node_block(), 0, lat->stream>>>(
+      static_cast<T*>(lat->pop), static_cast<T*>(lat->compact.cpop), a, lat->g);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(e, "compact exit launch");
+  return MLBM_OK;
+}
+
+template <typename T, int PHASE, int OUT>
+const void* step_fn() {
+  return reinterpret_cast<const void*>(&k_compact_step<T, PHASE, OUT>);
+}
+
+template <typename T>
+const void* pick_step(int phase, int out) {
+  if (phase == 0) {
+    switch (out) {
+      case OUT_NONE: return step_fn<T, 0, OUT_NONE>();
+      case OUT_RHO: return step_fn<T, 0, OUT_RHO>();
+      default: return step_fn<T, 0, OUT_RHO | OUT_VEL>();
+    }
+  }
+  switch (out) {
+    case OUT_NONE: return step_fn<T, 1, OUT_NONE>();
+    case OUT_RHO: return step_fn<T, 1, OUT_RHO>();
+    default: return step_fn<T, 1, OUT_RHO | OUT_VEL>();
+  }
+}
+
+template <typename T>
+mlbm_status set_smem_attr(size_t smem) {
+  for (int ph = 0; ph < 2; ++ph)
+    for (int out : {(int)OUT_NONE, (int)OUT_RHO, (int)(OUT_RHO | OUT_VEL)}) {
+      cudaError_t e = cudaFuncSetAttribute(pick_step<T>(ph, out),
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)smem);
+      if (e != cudaSuccess) return cuda_fail(e, "compact step attribute");
+    }
+  return MLBM_OK;
+}
+
+}  // namespace
+
+bool compact_supported(int lx, int ly, int lz, int storage) {
+  if (storage == MLBM_STORE_F64) return false;
+  if (ly < 4 || lz < 4 || lx > 65535) return false;
+  const Geom g = make_geom(lx, ly, lz);
+  return compact_smem_bytes(2, lx, g.wpr) <= kSmemMax;
+}
+
+mlbm_status compact_set_shape(mlbm_lattice* lat, int rows, int planes) {
+  CompactState& c = lat->compact;
+  const int old_rows = c.rows, old_planes = c.planes;
+  c.rows = rows;
+  c.planes = planes;
+  if (!c.built) return MLBM_OK;
+  if (mlbm_status st = build_tiling(lat)) {
+    c.rows = old_rows;
+    c.planes = old_planes;
+    build_tiling(lat);
+    return st;
+  }
+  // the parts of the last step follow the old tiling: take them again from
+  // the populations
+  if (c.active) {
+    if (mlbm_status st = compact_leave(lat)) return st;
+    return compact_enter(lat);
+  }
+  return MLBM_OK;
+}
+
+mlbm_status compact_enter(mlbm_lattice* lat) {
+  CompactState& c = lat->compact;
+  if (c.active) return MLBM_OK;
+  if (!c.supported)
+    return set_error(MLBM_ERR_ARG, "compact step does not support this lattice");
+  if (!c.built)
+    if (mlbm_status st = build_tables(lat)) return st;
+  mlbm_status st;
+  switch (lat->storage) {
+    case MLBM_STORE_F32: st = enter_t<float>(lat); break;
+    default: st = enter_t<__half>(lat); break;
+  }
+  if (st) return st;
+  c.active = true;
+  return MLBM_OK;
+}
+
+mlbm_status compact_sync_dense(mlbm_lattice* lat) {
+  if (!lat->compact.active) return MLBM_OK;
+  switch (lat->storage) {
+    case MLBM_STORE_F32: return to_dense_t<float>(lat);
+    default: return to_dense_t<__half>(lat);
+  }
+}
+
+mlbm_status compact_leave(mlbm_lattice* lat) {
+  if (!lat->compact.active) return MLBM_OK;
+  if (mlbm_status st = compact_sync_dense(lat)) return st;
+  lat->compact.active = false;
+  return MLBM_OK;
+}
+
+void compact_invalidate(mlbm_lattice* lat) {
+  lat->compact.built = false;
+  lat->compact.active = false;
+}
+
+void compact_free(mlbm_lattice* lat) {
+  CompactState& c = lat->compact;
+  cudaFree(c.cpop);
+  cudaFree(c.part);
+  cudaFree(c.wbase);
+  cudaFree(c.tabs);
+  c = CompactState{};
+}
+
+// The dynamic shared-memory limit is an attribute of the kernel on each
+// device: raise it (never lower it) to the largest size any lattice needs.
+template <typename T>
+mlbm_status ensure_smem_attr(int device, size_t smem) {
+  constexpr int kDevices = 64;
+  static std::mutex mu;
+  static size_t granted[kDevices] = {};
+  if (device < 0 || device >= kDevices)
+    return set_error(MLBM_ERR_ARG, "device index out of range");
+  std::lock_guard<std::mutex> lock(mu);
+  if (granted[device] >= smem) return MLBM_OK;
+  if (mlbm_status st = set_smem_attr<T>(smem)) return st;
+  granted[device] = smem;
+  return MLBM_OK;
+}
+
+template <typename T>
+mlbm_status launch_compact(mlbm_lattice* lat, const StepArgs& a, int out) {
+  CompactState& c = lat->compact;
+  if (mlbm_status st = ensure_smem_attr<T>(lat->device, c.smem)) return st;
+  T* cpop = static_cast<T*>(c.cpop);
+  float* rho = static_cast<float*>(lat->rho);
+  float* psi = static_cast<float*>(lat->psi);
+  float* vel = lat->vel;
+  Geom g = lat->g;
+  Phys p = lat->phys;
+  StepArgs aa = a;
+  CArgs cc = args_of(lat);
+  void* args[] = {&cpop, &cc, &rho, &psi, &vel, &g, &p, &aa};
+  cudaError_t e = cudaLaunchKernel(pick_step<T>(lat->phase, out),
+                                   dim3(c.nty * c.nzc), dim3(kThreads), args,
+                                   c.smem, lat->stream);
+  if (e != cudaSuccess) return cuda_fail(e, "compact time-step launch");
+  return MLBM_OK;
+}
+
+template mlbm_status launch_compact<float>(mlbm_lattice*, const StepArgs&, int);
+template mlbm_status launch_compact<__half>(mlbm_lattice*, const StepArgs&, int);
+
+}  // namespace mlbm

@@ -32,6 +32,9 @@
 namespace mlbm {
 
 constexpr uint32_t NB_SELF = 1u;
+
+// Output flags of one step launch: rho and psi fields, velocity field.
+enum { OUT_NONE = 0, OUT_RHO = 1, OUT_VEL = 2 };
 __host__ __device__ constexpr int nb_kind(uint32_t nb) { return (nb >> 19) & 3; }
 
 // Neighbour indices of one node: the index of (x+dx, y+dy, z+dz) is

@@ -50,9 +50,6 @@ struct March {
   long long budget_cycles;
 };
 
-// Output flags of one launch.
-enum { OUT_NONE = 0, OUT_RHO = 1, OUT_VEL = 2 };
-
 __device__ __forceinline__ unsigned ld_acquire(const unsigned* p) {
   unsigned v;
   asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");

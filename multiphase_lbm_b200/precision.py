@@ -33,15 +33,16 @@ import numpy as np
 
 from . import capi, host
 
-def drainage_params(shape, G=-5.0, g_ads=-1.0, rho_shift=1.0) -> capi.Params:
+def drainage_params(shape, G=-5.0, g_ads=-1.0, rho_shift=1.0,
+                     rho_inlet=0.10, rho_outlet=1.95) -> capi.Params:
     """Drainage case parameters; rhos from G_ads = G psi(rhos)."""
     import math
     lx = shape[0]
     rhos = -math.log(1.0 - g_ads / G)
     return capi.default_params(G=G, tau=1.0, rhos=rhos,
                                inlet_width=max(1, round(8 * lx / 200)),
-                               outlet_width=1, rho_inlet=0.10,
-                               rho_outlet=1.95, rho_shift=rho_shift)
+                               outlet_width=1, rho_inlet=rho_inlet,
+                               rho_outlet=rho_outlet, rho_shift=rho_shift)
 
 
 def interface_position(lat: capi.Lattice, inlet_width: int) -> int:
@@ -54,10 +55,12 @@ def interface_position(lat: capi.Lattice, inlet_width: int) -> int:
 
 
 def run(shape=(384, 384, 384), steps=10000, stat_every=500, seed=384,
-        device=0, G=-5.0, log=print) -> dict:
+        device=0, G=-5.0, rho_init=2.0, rho_inlet=0.10, rho_outlet=1.95,
+        log=print) -> dict:
     fluid, spheres = host.generate_packing(shape, 5.0, 15.0, 0.50, seed)
-    rho0 = np.full(shape, 2.0, np.float32)
-    params = drainage_params(shape, G=G)
+    rho0 = np.full(shape, rho_init, np.float32)
+    params = drainage_params(shape, G=G, rho_inlet=rho_inlet,
+                             rho_outlet=rho_outlet)
     formats = {"f64": capi.STORE_F64, "f32": capi.STORE_F32,
                "f16": capi.STORE_F16}
     lats = {}
@@ -89,6 +92,8 @@ def run(shape=(384, 384, 384), steps=10000, stat_every=500, seed=384,
     s64 = lats["f64"].stats()
     x64 = interface_position(lats["f64"], params.inlet_width)
     report = {"lattice": list(shape), "steps": steps, "G": G,
+              "rho_init": rho_init, "rho_inlet": rho_inlet,
+              "rho_outlet": rho_outlet,
               "fluid_nodes": int(m.sum()),
               "spheres": int(len(spheres)), "elapsed_s": round(elapsed, 1),
               "formats": {}}
@@ -119,10 +124,14 @@ def main(argv=None) -> int:
     ap.add_argument("--stat-every", type=int, default=500)
     ap.add_argument("--seed", type=int, default=384)
     ap.add_argument("--G", type=float, default=-5.0)
+    ap.add_argument("--rho-init", type=float, default=2.0)
+    ap.add_argument("--rho-inlet", type=float, default=0.10)
+    ap.add_argument("--rho-outlet", type=float, default=1.95)
     ap.add_argument("--out", default="")
     a = ap.parse_args(argv)
     rep = run((a.size,) * 3, a.steps, a.stat_every, a.seed, G=a.G,
-              log=lambda s: print(s, file=sys.stderr, flush=True))
+              rho_init=a.rho_init, rho_inlet=a.rho_inlet,
+              rho_outlet=a.rho_outlet, log=lambda s: print(s, file=sys.stderr, flush=True))
     text = json.dumps(rep, indent=1)
     if a.out:
         with open(a.out, "w") as fh:

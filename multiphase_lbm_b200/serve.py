@@ -158,8 +158,11 @@ def serve_batched(reqs, hbm_cap=150e9, chunk=CONVERGENCE_STEPS, log=None):
     return makespan, reqs
 
 
-def serve_fifo(reqs, chunk=CONVERGENCE_STEPS, log=None):
-    """Requests one at a time in arrival order, each alone on the GPU."""
+def serve_fifo(reqs, chunk=CONVERGENCE_STEPS, log=None,
+               kernel=capi.KERNEL_TWO_PASS):
+    """Requests one at a time in arrival order, each alone on the GPU, with
+    the batch's two-pass kernels by default (then every result equals the
+    batched one bit for bit)."""
     t0 = time.perf_counter()
     for r in sorted(reqs, key=lambda q: q.arrival):
         now = time.perf_counter() - t0
@@ -168,6 +171,7 @@ def serve_fifo(reqs, chunk=CONVERGENCE_STEPS, log=None):
         fl, rho, p = geometry(r)
         lat = capi.Lattice(r.shape, storage=capi.STORE_F16 if r.fp16_ok
                            else capi.STORE_F32)
+        lat.set_step_kernel(kernel)
         lat.set_params(p)
         lat.upload(fl, rho)
         lat.initialize()
@@ -203,6 +207,8 @@ def main(argv=None) -> int:
     ap.add_argument("--hbm-cap-gb", type=float, default=150.0)
     ap.add_argument("--seed", type=int, default=7)
     ap.add_argument("--no-fifo", action="store_true")
+    ap.add_argument("--fifo-kernel", default="two-pass",
+                    choices=["two-pass", "compact"])
     a = ap.parse_args(argv)
     log = lambda s: print(s, file=sys.stderr, flush=True)  # noqa: E731
     reqs = make_requests(a.requests, a.rate, a.seed, a.budget_scale)
@@ -213,7 +219,10 @@ def main(argv=None) -> int:
            "batched": summarise(mk, done)}
     if not a.no_fifo:
         reqs2 = make_requests(a.requests, a.rate, a.seed, a.budget_scale)
-        mk2, done2 = serve_fifo(reqs2, log=log)
+        kern = (capi.KERNEL_TWO_PASS if a.fifo_kernel == "two-pass"
+                else capi.KERNEL_COMPACT)
+        mk2, done2 = serve_fifo(reqs2, log=log, kernel=kern)
+        out["fifo_kernel"] = a.fifo_kernel
         out["fifo"] = summarise(mk2, done2)
         same = [abs(x.saturation - y.saturation) <= 0.0 and x.steps == y.steps
                 for x, y in zip(sorted(done, key=lambda r: r.rid),

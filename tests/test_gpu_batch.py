@@ -17,7 +17,9 @@ def _params(capi, i, shape):
 
 
 def _alone(capi, shape, fluid, rho, params, storage, steps):
+    # the batch advances the dense layout with the two-pass kernels
     lat = capi.Lattice(shape, storage=storage)
+    lat.set_step_kernel(capi.KERNEL_TWO_PASS)
     lat.set_params(params)
     lat.upload(fluid, rho)
     lat.initialize()

@@ -1,0 +1,158 @@
+"""The single-pass step over the compact (fluid-only) layout.
+
+Its collision is the two-pass collision; psi of the next step is formed from
+fixed-point part sums of the post-collision populations instead of a second
+pass, so it agrees with the reference's kernels (the oracle) to rounding.
+Tolerances (the FP32 parity bar): density within 1e-5 relative pointwise,
+populations and velocity within 1e-5 relative to their largest value, over
+the first 100 steps; FP16 storage: density within 2e-3 relative.
+"""
+import numpy as np
+import pytest
+
+import oracle
+from conftest import pointwise_rel_err, rel_err, sphere_case
+
+pytestmark = pytest.mark.gpu
+
+DRAIN = dict(G=-5.0, rhos=0.223144, tau=1.0, inlet_width=3, outlet_width=1,
+             rho_inlet=0.17, rho_outlet=1.90)
+
+
+def _lattice(capi, shape, fluid, rho, kernel, storage=0, shape_kc=None, **kw):
+    lat = capi.Lattice(shape, storage=storage)
+    lat.set_step_kernel(kernel)
+    if shape_kc:
+        lat.set_compact_shape(*shape_kc)
+    lat.set_params(capi.default_params(**kw))
+    lat.upload(fluid, rho)
+    lat.initialize()
+    return lat
+
+
+def test_compact_matches_oracle_drainage_100_steps():
+    from multiphase_lbm_b200 import capi
+    shape = (64, 48, 40)
+    fluid, rho = sphere_case(shape, seed=11, rmin=3.0, rmax=6.0, porosity=0.55,
+                             rho0=1.9, amp=0.02)
+    lat = _lattice(capi, shape, fluid, rho, capi.KERNEL_COMPACT, **DRAIN)
+    port = oracle.Port(rho, fluid, oracle.make_params(**DRAIN))
+    m = fluid.astype(bool)
+    step = 0
+    for n in (1, 9, 89):
+        lat.iterate(step, n)
+        port.step(step, n)
+        step += n
+        e = pointwise_rel_err(lat.field("rho"), port.get("rho"), m)
+        assert e <= 1e-5, f"step {step}: rho {e:.3e}"
+        e = rel_err(lat.field("f"), port.get("f"), m)
+        assert e <= 1e-5, f"step {step}: populations {e:.3e}"
+    lat.iterate(step, 1, write_velocity=True)
+    port.step(step, 1)
+    e = rel_err(lat.field("velocity")[m], port.get("velocity")[m])
+    assert e <= 1e-5, f"velocity {e:.3e}"
+
+
+# lattice shapes x compact tilings: uneven splits, exactly two tiles along y
+# or z, rows longer than one mask word, odd row lengths
+CASES = [((40, 32, 24), (4, 8)), ((33, 5, 7), (2, 2)), ((70, 9, 4), (4, 2)),
+         ((100, 12, 13), (3, 5)), ((48, 16, 16), (8, 8)), ((300, 6, 6), (3, 3))]
+
+
+@pytest.mark.parametrize("shape,kc", CASES)
+def test_compact_agrees_with_two_pass(shape, kc):
+    from multiphase_lbm_b200 import capi
+    fluid, rho = sphere_case(shape, seed=sum(shape), rmin=1.5, rmax=3.5,
+                             porosity=0.6, rho0=0.7, amp=0.1)
+    kw = dict(G=-5.0, rhos=0.223144, tau=1.0)
+    a = _lattice(capi, shape, fluid, rho, capi.KERNEL_COMPACT, shape_kc=kc, **kw)
+    b = _lattice(capi, shape, fluid, rho, capi.KERNEL_TWO_PASS, **kw)
+    m = fluid.astype(bool)
+    for s0, n in ((0, 1), (1, 2), (3, 47)):
+        a.iterate(s0, n)
+        b.iterate(s0, n)
+        e = pointwise_rel_err(a.field("rho"), b.field("rho"), m)
+        assert e <= 1e-5, f"{shape} {kc} step {s0 + n}: rho {e:.3e}"
+        e = rel_err(a.field("f"), b.field("f"), m)
+        assert e <= 1e-5, f"{shape} {kc} step {s0 + n}: populations {e:.3e}"
+
+
+def test_compact_fp16_close_to_two_pass_fp16():
+    from multiphase_lbm_b200 import capi
+    shape = (48, 40, 32)
+    fluid, rho = sphere_case(shape, seed=4, rmin=2.0, rmax=5.0, porosity=0.55,
+                             rho0=1.9, amp=0.02)
+    kw = dict(DRAIN, rho_shift=1.0)
+    a = _lattice(capi, shape, fluid, rho, capi.KERNEL_COMPACT,
+                 storage=capi.STORE_F16, **kw)
+    b = _lattice(capi, shape, fluid, rho, capi.KERNEL_TWO_PASS,
+                 storage=capi.STORE_F16, **kw)
+    a.iterate(0, 100)
+    b.iterate(0, 100)
+    m = fluid.astype(bool)
+    e = pointwise_rel_err(a.field("rho"), b.field("rho"), m)
+    assert e <= 2e-3, f"fp16 rho {e:.3e}"
+
+
+def test_compact_deterministic_bitwise():
+    from multiphase_lbm_b200 import capi
+    shape = (64, 32, 32)
+    fluid, rho = sphere_case(shape, seed=9, rmin=2.0, rmax=5.0, porosity=0.5,
+                             rho0=0.7, amp=0.05)
+    outs = []
+    for _ in range(2):
+        lat = _lattice(capi, shape, fluid, rho, capi.KERNEL_AUTO,
+                       G=-6.0, rhos=0.182322)
+        lat.iterate(0, 60)
+        outs.append((lat.field("rho"), lat.field("f")))
+    assert np.array_equal(outs[0][0], outs[1][0])
+    assert np.array_equal(outs[0][1], outs[1][1])
+
+
+def test_kernel_switching_keeps_the_state():
+    """compact -> two-pass -> compact, against two-pass throughout."""
+    from multiphase_lbm_b200 import capi
+    shape = (40, 24, 20)
+    fluid, rho = sphere_case(shape, seed=2, rmin=2.0, rmax=4.0, porosity=0.6,
+                             rho0=1.9, amp=0.02)
+    a = _lattice(capi, shape, fluid, rho, capi.KERNEL_COMPACT, **DRAIN)
+    b = _lattice(capi, shape, fluid, rho, capi.KERNEL_TWO_PASS, **DRAIN)
+    step = 0
+    for kind in (capi.KERNEL_COMPACT, capi.KERNEL_TWO_PASS,
+                 capi.KERNEL_COMPACT, capi.KERNEL_FUSED):
+        a.set_step_kernel(kind)
+        a.iterate(step, 15)
+        b.iterate(step, 15)
+        step += 15
+    m = fluid.astype(bool)
+    assert pointwise_rel_err(a.field("rho"), b.field("rho"), m) <= 1e-5
+    assert rel_err(a.field("f"), b.field("f"), m) <= 1e-5
+
+
+def test_compact_shape_and_autotune():
+    from multiphase_lbm_b200 import capi
+    shape = (64, 32, 32)
+    fluid, rho = sphere_case(shape, seed=5, rmin=2.0, rmax=5.0, porosity=0.5,
+                             rho0=1.9, amp=0.02)
+    a = _lattice(capi, shape, fluid, rho, capi.KERNEL_COMPACT, **DRAIN)
+    b = _lattice(capi, shape, fluid, rho, capi.KERNEL_TWO_PASS, **DRAIN)
+    rows, planes, done = a.autotune(0, trial_steps=2)
+    assert 2 <= rows <= 8 and 2 <= planes <= 32 and done > 0
+    b.iterate(0, done)
+    a.set_compact_shape(3, 5)          # reshaped while the state is compact
+    a.iterate(done, 10)
+    b.iterate(done, 10)
+    m = fluid.astype(bool)
+    assert pointwise_rel_err(a.field("rho"), b.field("rho"), m) <= 1e-5
+    with pytest.raises(capi.MlbmError):
+        a.set_compact_shape(1, 8)      # tiles need two rows at least
+
+
+def test_compact_rejects_fp64_and_flat_lattices():
+    from multiphase_lbm_b200 import capi
+    lat = capi.Lattice((16, 16, 16), storage=capi.STORE_F64)
+    with pytest.raises(capi.MlbmError):
+        lat.set_step_kernel(capi.KERNEL_COMPACT)
+    lat = capi.Lattice((16, 3, 16))
+    with pytest.raises(capi.MlbmError):
+        lat.set_step_kernel(capi.KERNEL_COMPACT)

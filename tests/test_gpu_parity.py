@@ -19,14 +19,18 @@ from conftest import pointwise_rel_err, random_case, rel_err, sphere_case
 pytestmark = pytest.mark.gpu
 
 SC_PARAMS = dict(G=-6.0, rhos=0.182322, tau=1.0)
+# the default kernel (the compact single-pass step where supported) and the
+# two-pass kernels
+KERNELS = [0, 2]
 
 
-def _pair(shape, fluid, rho, storage=0, f64_oracle=False, **kw):
+def _pair(shape, fluid, rho, storage=0, f64_oracle=False, kernel=0, **kw):
     from multiphase_lbm_b200 import capi
     p = capi.default_params(**kw)
     op = oracle.make_params(**{k: v for k, v in kw.items()
                                if k not in ("rho_shift",)})
     lat = capi.Lattice(shape, storage=storage)
+    lat.set_step_kernel(kernel)
     lat.set_params(p)
     lat.upload(fluid, rho)
     lat.initialize()
@@ -45,10 +49,11 @@ def _compare(lat, port, fluid, tol_rho, tol_f, label, f64=False):
     return e_rho, e_f
 
 
+@pytest.mark.parametrize("kernel", KERNELS)
 @pytest.mark.parametrize("shape", [(24, 20, 18), (33, 7, 5), (64, 9, 3)])
-def test_periodic_random_mask_fp32(shape):
+def test_periodic_random_mask_fp32(shape, kernel):
     fluid, rho = random_case(shape, seed=sum(shape))
-    lat, port = _pair(shape, fluid, rho, **SC_PARAMS)
+    lat, port = _pair(shape, fluid, rho, kernel=kernel, **SC_PARAMS)
     step = 0
     for n in (1, 9, 90):
         lat.iterate(step, n)
@@ -57,11 +62,13 @@ def test_periodic_random_mask_fp32(shape):
         _compare(lat, port, fluid, 1e-5, 1e-5, f"{shape} step {step}")
 
 
-def test_sphere_packing_64_fp32_100_steps():
-    """Config-0 physics (G=-6, G_ads=-1 -> rhos=0.182322, rho 0.70+-0.01)."""
+@pytest.mark.parametrize("kernel", KERNELS)
+def test_sphere_packing_64_fp32_100_steps(kernel):
+    """Phase separation on a 64^3 packing (G=-6, G_ads=-1 -> rhos=0.182322,
+    rho 0.70+-0.01)."""
     shape = (64, 64, 64)
     fluid, rho = sphere_case(shape, seed=7)
-    lat, port = _pair(shape, fluid, rho, **SC_PARAMS)
+    lat, port = _pair(shape, fluid, rho, kernel=kernel, **SC_PARAMS)
     lat.iterate(0, 99)
     port.step(0, 99)
     lat.iterate(99, 1, write_velocity=True)
@@ -73,13 +80,14 @@ def test_sphere_packing_64_fp32_100_steps():
     assert e <= 1e-5, f"velocity rel err {e:.3e}"
 
 
-def test_drainage_boundary_fp32():
+@pytest.mark.parametrize("kernel", KERNELS)
+def test_drainage_boundary_fp32(kernel):
     shape = (40, 24, 20)
     fluid, rho = sphere_case(shape, seed=3, rmin=2.0, rmax=4.0, porosity=0.6,
                              rho0=2.0, amp=0.0)
     kw = dict(SC_PARAMS, inlet_width=3, outlet_width=1, rho_inlet=0.10,
               rho_outlet=1.95)
-    lat, port = _pair(shape, fluid, rho, **kw)
+    lat, port = _pair(shape, fluid, rho, kernel=kernel, **kw)
     step = 0
     for n in (1, 9, 90):
         lat.iterate(step, n)
@@ -88,13 +96,14 @@ def test_drainage_boundary_fp32():
         _compare(lat, port, fluid, 1e-5, 1e-5, f"drainage step {step}")
 
 
+@pytest.mark.parametrize("kernel", KERNELS)
 @pytest.mark.parametrize("inject_type,reverse", [(0, 1), (1, 1), (2, -1)])
-def test_injection_fp32(inject_type, reverse):
+def test_injection_fp32(inject_type, reverse, kernel):
     shape = (24, 20, 18)
     fluid, rho = random_case(shape, seed=11, rho0=0.5, amp=0.3)
     kw = dict(SC_PARAMS, rho_increment=0.01, rho_inject_period=3,
               inject_position=0.5, inject_density=1)
-    lat, port = _pair(shape, fluid, rho, **kw)
+    lat, port = _pair(shape, fluid, rho, kernel=kernel, **kw)
     lat.iterate(0, 30, reverse=reverse, inject_type=inject_type)
     port.step(0, 30, reverse=reverse, inject_type=inject_type)
     _compare(lat, port, fluid, 1e-5, 1e-5, f"inject {inject_type}")
@@ -141,11 +150,12 @@ def test_fp16_storage_close_to_fp64_oracle():
     assert e <= 2e-3, e
 
 
-def test_all_fluid_and_all_solid_edges():
+@pytest.mark.parametrize("kernel", KERNELS)
+def test_all_fluid_and_all_solid_edges(kernel):
     shape = (16, 8, 8)
     rho = np.full(shape, 0.7, np.float32)
     for fl in (np.ones(shape, np.uint8), np.zeros(shape, np.uint8)):
-        lat, port = _pair(shape, fl, rho, **SC_PARAMS)
+        lat, port = _pair(shape, fl, rho, kernel=kernel, **SC_PARAMS)
         lat.iterate(0, 5)
         port.step(0, 5)
         if fl.any():
