@@ -81,7 +81,8 @@ def load_traffic(kernel, storage):
 
 
 # roofline label and launches per step of each step kernel
-KERNEL_INFO = {3: ("compact", "k_compact_step (single pass, compact layout)", 1),
+KERNEL_INFO = {4: ("single-pass", "k_compact_step (single pass, compact layout)", 1),
+               3: ("compact", "time step (k_cdensity + k_cupdate, compact layout)", 2),
                2: ("two-pass", "time step (k_density + k_update_zm)", 2),
                1: ("fused", "k_step_fused (persistent)", 1)}
 
@@ -220,7 +221,7 @@ def main():
     ap.add_argument("--size", type=int, default=200,
                     help="lattice edge (profiling runs use a smaller case)")
     ap.add_argument("--kernel", default="auto",
-                    choices=["auto", "compact", "fused", "two-pass"])
+                    choices=["auto", "compact", "single-pass", "fused", "two-pass"])
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -251,6 +252,7 @@ def main():
     lat.upload(fluid, rho)
     lat.initialize()
     kernel_id = {"auto": capi.KERNEL_AUTO, "compact": capi.KERNEL_COMPACT,
+                 "single-pass": capi.KERNEL_SINGLE_PASS,
                  "fused": capi.KERNEL_FUSED,
                  "two-pass": capi.KERNEL_TWO_PASS}[args.kernel]
     lat.set_step_kernel(kernel_id)

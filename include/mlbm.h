@@ -173,29 +173,34 @@ mlbm_status mlbm_iterate(mlbm_lattice* lat, int64_t step0, int32_t nsteps,
                          uint32_t flags);
 
 /* Which kernels advance the lattice:
- *   TWO_PASS  a density launch and an update launch per step over the dense
- *             layout; bit-identical to the reference's kernels;
- *   FUSED     one cooperative launch per step, the two passes interleaved
- *             plane by plane; bit-identical to TWO_PASS;
- *   COMPACT   one launch per step over a fluid-only population layout: the
- *             populations are read and written once per step and psi of the
- *             next step is accumulated from the outputs.  FP32 / FP16 storage,
- *             ly, lz >= 4.  The collision is the same; psi is formed from a
- *             differently ordered sum of the same populations, so results
- *             agree with TWO_PASS to rounding (not bit for bit) and are
- *             deterministic;
- *   AUTO      (default) COMPACT where supported, else TWO_PASS.
+ *   TWO_PASS     a density launch and an update launch per step over the
+ *                dense layout; bit-identical to the reference's kernels;
+ *   FUSED        one cooperative launch per step, the two passes interleaved
+ *                plane by plane; bit-identical to TWO_PASS;
+ *   COMPACT      the two passes over a fluid-only population layout (solid
+ *                nodes own no population storage), one thread per fluid
+ *                node; bit-identical to TWO_PASS.  FP32 / FP16 storage, at
+ *                most 2048 x 2048 x 1024 nodes;
+ *   SINGLE_PASS  one launch per step over the fluid-only layout: the
+ *                populations are read and written once per step and psi of
+ *                the next step is accumulated from the outputs.  FP32 / FP16
+ *                storage, ly, lz >= 4.  The collision is the same; psi is
+ *                formed from a differently ordered sum of the same
+ *                populations, so results agree with TWO_PASS to rounding (not
+ *                bit for bit) and are deterministic;
+ *   AUTO         (default) COMPACT where supported, else TWO_PASS.
  * The state moves between the layouts on demand (the dense buffers stay
- * allocated; COMPACT adds 19 populations and 4 partial sums per fluid node,
- * allocated on first use). */
+ * allocated; the fluid-only layout adds 19 populations and 14 words per
+ * fluid node, allocated on first use). */
 #define MLBM_KERNEL_AUTO 0
 #define MLBM_KERNEL_FUSED 1
 #define MLBM_KERNEL_TWO_PASS 2
 #define MLBM_KERNEL_COMPACT 3
+#define MLBM_KERNEL_SINGLE_PASS 4
 mlbm_status mlbm_set_step_kernel(mlbm_lattice* lat, int32_t kind);
 /* The kernel the next mlbm_iterate runs (AUTO resolved); -1 for NULL. */
 int32_t mlbm_get_step_kernel(const mlbm_lattice* lat);
-/* Tiling of the COMPACT step: a block walks `rows` full x-rows (y) through
+/* Tiling of the SINGLE_PASS step: a block walks `rows` full x-rows (y) through
  * `planes` planes (z); at least two tiles along y and z, each at least two
  * rows / planes deep.  Default 4 x 8. */
 mlbm_status mlbm_set_compact_shape(mlbm_lattice* lat, int32_t rows,
@@ -210,7 +215,8 @@ mlbm_status mlbm_set_tuning(mlbm_lattice* lat, int32_t rows_per_item,
 mlbm_status mlbm_set_update_shape(mlbm_lattice* lat, int32_t rows,
                                   int32_t planes);
 /* Time candidate shapes of the lattice's step kernel (update shape for
- * TWO_PASS, tiling for COMPACT) and keep the fastest.  The trial steps are
+ * TWO_PASS, tiling for SINGLE_PASS; COMPACT has none: out = {0, 0}, no
+ * steps) and keep the fastest.  The trial steps are
  * real steps (step0, step0+1, ...): the lattice advances by *steps_done of
  * them.  out (optional, 2 ints) receives rows, planes. */
 mlbm_status mlbm_autotune(mlbm_lattice* lat, int64_t step0,

@@ -20,7 +20,8 @@ FIELD_RHO, FIELD_PRESSURE, FIELD_PSI, FIELD_VELOCITY, FIELD_POPULATIONS, \
     FIELD_FLUID = range(6)
 DTYPE_F32, DTYPE_F64, DTYPE_U8 = 0, 1, 2
 ITER_WRITE_VELOCITY = 1
-KERNEL_AUTO, KERNEL_FUSED, KERNEL_TWO_PASS, KERNEL_COMPACT = 0, 1, 2, 3
+KERNEL_AUTO, KERNEL_FUSED, KERNEL_TWO_PASS, KERNEL_COMPACT, KERNEL_SINGLE_PASS = \
+    0, 1, 2, 3, 4
 Q = 19
 
 STATUS = {0: "MLBM_OK", 1: "MLBM_ERR_ARG", 2: "MLBM_ERR_CUDA",
@@ -196,7 +197,7 @@ class Lattice:
         return int(lib().mlbm_get_step_kernel(self.h))
 
     def set_compact_shape(self, rows: int = 4, planes: int = 8) -> None:
-        """Tiling of the compact step (rows along y, planes along z)."""
+        """Tiling of the single-pass step (rows along y, planes along z)."""
         check(lib().mlbm_set_compact_shape(self.h, rows, planes))
 
     def autotune(self, step0: int, trial_steps: int = 4):

@@ -209,7 +209,7 @@ mlbm_status launch_two_pass(mlbm_lattice* lat, const StepArgs& a, bool wu,
 // it supports the lattice (FP32 / FP16 storage), else the two-pass step.
 int effective_kernel(const mlbm_lattice* lat) {
   if (lat->step_kernel != MLBM_KERNEL_AUTO) return lat->step_kernel;
-  return lat->compact.supported ? MLBM_KERNEL_COMPACT : MLBM_KERNEL_TWO_PASS;
+  return lat->compact.two_pass_ok ? MLBM_KERNEL_COMPACT : MLBM_KERNEL_TWO_PASS;
 }
 
 template <typename T>
@@ -220,14 +220,25 @@ mlbm_status launch_steps(mlbm_lattice* lat, int64_t step0, int32_t nsteps,
   const bool fused = kind == MLBM_KERNEL_FUSED && lat->fused.ok;
   if (kind == MLBM_KERNEL_FUSED && !lat->fused.ok)
     return fail(MLBM_ERR_ARG, "fused kernel does not fit this lattice");
-  bool compact = false;
-  if constexpr (!std::is_same<T, double>::value) compact = kind == MLBM_KERNEL_COMPACT;
+  bool compact = false, single = false;
+  if constexpr (!std::is_same<T, double>::value) {
+    compact = kind == MLBM_KERNEL_COMPACT || kind == MLBM_KERNEL_SINGLE_PASS;
+    single = kind == MLBM_KERNEL_SINGLE_PASS;
+  }
   if ((flags & MLBM_ITER_WRITE_VELOCITY) && !lat->vel) {
     // the velocity field is allocated on first request
     CUDA_TRY(cudaMalloc((void**)&lat->vel, (size_t)lat->g.plane * 3 * sizeof(float)),
              "velocity allocation");
+    // solid nodes are never written: they read zero velocity
+    CUDA_TRY(cudaMemsetAsync(lat->vel, 0, (size_t)lat->g.plane * 3 * sizeof(float),
+                             lat->stream),
+             "velocity clear");
   }
   if (compact) {
+    // the single-pass step reads the part sums of the step before it: take
+    // them again from the populations if another kernel ran last
+    if (single && lat->compact.active && !lat->compact.parts_valid)
+      if (mlbm_status st = compact_leave(lat)) return st;
     if (mlbm_status st = compact_enter(lat)) return st;
   } else {
     if (mlbm_status st = compact_leave(lat)) return st;
@@ -239,9 +250,11 @@ mlbm_status launch_steps(mlbm_lattice* lat, int64_t step0, int32_t nsteps,
     const int out = wu ? (OUT_RHO | OUT_VEL) : (last ? OUT_RHO : OUT_NONE);
     mlbm_status st;
     if constexpr (!std::is_same<T, double>::value) {
-      if (compact) st = launch_compact<T>(lat, a, out);
+      if (single) st = launch_compact<T>(lat, a, out);
+      else if (compact) st = launch_compact_two_pass<T>(lat, a, wu, last);
       else if (fused) st = launch_fused<T>(lat, a, out);
       else st = launch_two_pass<T>(lat, a, wu, last);
+      lat->compact.parts_valid = single;
     } else {
       if (fused) st = launch_fused<T>(lat, a, out);
       else st = launch_two_pass<T>(lat, a, wu, last);
@@ -419,6 +432,7 @@ mlbm_status mlbm_lattice_create(int32_t lx, int32_t ly, int32_t lz,
   lat->g = make_geom(lx, ly, lz);
   lat->fused = fused_shape(lat->g, storage, 0, 0);
   lat->compact.supported = compact_supported(lx, ly, lz, storage);
+  lat->compact.two_pass_ok = compact_two_pass_supported(lx, ly, lz, storage);
   const size_t np = (size_t)lat->g.plane;
   const size_t mask_words = (size_t)lz * ly * lat->g.wpr;
   cudaError_t e = cudaSuccess;
@@ -729,14 +743,18 @@ mlbm_status mlbm_plane_profile(mlbm_lattice* lat, int64_t* n_fluid_x,
 
 mlbm_status mlbm_set_step_kernel(mlbm_lattice* lat, int32_t kind) {
   if (mlbm_status st = check_lat(lat)) return st;
-  if (kind < MLBM_KERNEL_AUTO || kind > MLBM_KERNEL_COMPACT)
+  if (kind < MLBM_KERNEL_AUTO || kind > MLBM_KERNEL_SINGLE_PASS)
     return fail(MLBM_ERR_ARG, "invalid step kernel %d", kind);
   if (kind == MLBM_KERNEL_FUSED && !lat->fused.ok)
     return fail(MLBM_ERR_ARG, "fused kernel does not fit this lattice");
-  if (kind == MLBM_KERNEL_COMPACT && !lat->compact.supported)
+  if (kind == MLBM_KERNEL_COMPACT && !lat->compact.two_pass_ok)
     return fail(MLBM_ERR_ARG,
-                "compact step needs FP32 or FP16 storage, ly and lz >= 4 and "
-                "a row that fits shared memory");
+                "compact kernels need FP32 or FP16 storage and at most "
+                "2048 x 2048 x 1024 nodes");
+  if (kind == MLBM_KERNEL_SINGLE_PASS && !lat->compact.supported)
+    return fail(MLBM_ERR_ARG,
+                "single-pass step needs FP32 or FP16 storage, ly and lz >= 4 "
+                "and a row that fits shared memory");
   lat->step_kernel = kind;
   return MLBM_OK;
 }
@@ -788,7 +806,13 @@ mlbm_status mlbm_autotune(mlbm_lattice* lat, int64_t step0,
   if (!lat->initialized) return fail(MLBM_ERR_STATE, "autotune before initialize");
   if (trial_steps < 1) trial_steps = 2;
   if (mlbm_status st = activate(lat)) return st;
-  const bool compact = effective_kernel(lat) == MLBM_KERNEL_COMPACT;
+  if (effective_kernel(lat) == MLBM_KERNEL_COMPACT) {
+    // one thread per fluid node: nothing to tune
+    if (out) out[0] = out[1] = 0;
+    if (steps_done) *steps_done = 0;
+    return MLBM_OK;
+  }
+  const bool compact = effective_kernel(lat) == MLBM_KERNEL_SINGLE_PASS;
   const int rows_u[] = {1, 2, 4, 8};
   const int planes_u[] = {2, 4, 8, 16, 32};
   const int rows_k[] = {2, 3, 4, 6, 8};

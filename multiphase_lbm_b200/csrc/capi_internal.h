@@ -25,9 +25,13 @@ struct CompactState {
   bool supported = false;  // storage and lattice shape allow the step
   bool built = false;      // tables match the current mask
   bool active = false;     // the compact buffer holds the current state
+  bool parts_valid = false;  // part sums match the state (single-pass step)
   long long nfluid = 0, cs = 0;
   void* cpop = nullptr;        // [Q][cs] populations (T)
   float* part = nullptr;       // [2][4][cs] part sums of rho (two sets)
+  uint32_t* cnb = nullptr;     // [cs] neighbour words in compact order
+  uint2* cinfo = nullptr;      // [cs] (neighbour word, packed x, y, z)
+  bool two_pass_ok = false;    // the compact two-pass kernels fit the lattice
   uint32_t* wbase = nullptr;   // [rows * wpr + 1]
   int* tabs = nullptr;         // ytab[ly], ztab[lz], ystart[nty+1], zstart[nzc+1]
   long long cap = 0;           // cs the buffers were allocated for
@@ -98,4 +102,8 @@ void compact_invalidate(mlbm_lattice* lat);     // the mask changed
 void compact_free(mlbm_lattice* lat);
 template <typename T>
 mlbm_status launch_compact(mlbm_lattice* lat, const StepArgs& a, int out);
+template <typename T>
+mlbm_status launch_compact_two_pass(mlbm_lattice* lat, const StepArgs& a,
+                                    bool write_u, bool write_rho);
+bool compact_two_pass_supported(int lx, int ly, int lz, int storage);
 }  // namespace mlbm

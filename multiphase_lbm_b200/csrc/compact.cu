@@ -9,6 +9,7 @@
 
 #include "capi_internal.h"
 #include "compact.cuh"
+#include "compact2.cuh"
 
 namespace mlbm {
 
@@ -17,7 +18,6 @@ namespace {
 dim3 node_block() { return dim3(32, 4, 1); }
 dim3 node_grid(const Geom& g) { return dim3(g.px / 32, (g.ly + 3) / 4, g.lz); }
 
-constexpr int kThreads = 256;
 constexpr size_t kSmemMax = 227 * 1024;
 
 // Part buffers: two sets of [4][cs]; a step from AA phase `ph` reads set ph
@@ -29,6 +29,7 @@ CArgs args_of(const mlbm_lattice* lat) {
   CArgs a;
   a.mask = lat->mask;
   a.wbase = c.wbase;
+  a.cnb = c.cnb;
   a.ytab = c.tabs;
   a.ztab = c.tabs + g.ly;
   a.ystart = c.tabs + g.ly + g.lz;
@@ -122,14 +123,24 @@ mlbm_status build_tables(mlbm_lattice* lat) {
   if (c.cs > c.cap) {
     cudaFree(c.cpop);
     cudaFree(c.part);
+    cudaFree(c.cnb);
+    cudaFree(c.cinfo);
     c.cpop = nullptr;
     c.part = nullptr;
+    c.cnb = nullptr;
+    c.cinfo = nullptr;
     c.cap = 0;
     e = cudaMalloc(&c.cpop, (size_t)c.cs * Q * pop_elem_bytes(lat->storage));
     if (e == cudaSuccess) e = cudaMalloc((void**)&c.part, (size_t)c.cs * 8 * sizeof(float));
+    if (e == cudaSuccess) e = cudaMalloc((void**)&c.cnb, (size_t)c.cs * sizeof(uint32_t));
+    if (e == cudaSuccess) e = cudaMalloc((void**)&c.cinfo, (size_t)c.cs * sizeof(uint2));
     if (e != cudaSuccess) {
       cudaFree(c.cpop);
+      cudaFree(c.part);
+      cudaFree(c.cnb);
       c.cpop = nullptr;
+      c.part = nullptr;
+      c.cnb = nullptr;
       cudaGetLastError();
       return cuda_fail(e, "compact buffers");
     }
@@ -148,7 +159,10 @@ mlbm_status enter_t(mlbm_lattice* lat) {
   float* seed = c.part + (size_t)lat->phase * 4 * c.cs;
   a.part_wr = seed;
   k_convert<T, true><<<node_grid(lat->g), node_block(), 0, lat->stream>>>(
-      static_cast<T*>(lat->pop), static_cast<T*>(c.cpop), a, lat->g);
+      static_cast<T*>(lat->pop), static_cast<T*>(c.cpop), lat->nbw, c.cnb, a,
+      lat->g);
+  k_cinfo<<<node_grid(lat->g), node_block(), 0, lat->stream>>>(lat->nbw, c.cinfo,
+                                                                a, lat->g);
   cudaError_t e = cudaMemsetAsync(seed + c.cs, 0, 3 * c.cs * sizeof(float), lat->stream);
   if (e != cudaSuccess) return cuda_fail(e, "compact parts");
   if (lat->phase == 0)
@@ -166,7 +180,8 @@ template <typename T>
 mlbm_status to_dense_t(mlbm_lattice* lat) {
   const CArgs a = args_of(lat);
   k_convert<T, false><<<node_grid(lat->g), node_block(), 0, lat->stream>>>(
-      static_cast<T*>(lat->pop), static_cast<T*>(lat->compact.cpop), a, lat->g);
+      static_cast<T*>(lat->pop), static_cast<T*>(lat->compact.cpop), nullptr,
+      nullptr, a, lat->g);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(e, "compact exit launch");
   return MLBM_OK;
@@ -214,6 +229,11 @@ bool compact_supported(int lx, int ly, int lz, int storage) {
   return compact_smem_bytes(2, lx, g.wpr) <= kSmemMax;
 }
 
+bool compact_two_pass_supported(int lx, int ly, int lz, int storage) {
+  return storage != MLBM_STORE_F64 && lx <= kC2MaxX && ly <= kC2MaxY &&
+         lz <= kC2MaxZ;
+}
+
 mlbm_status compact_set_shape(mlbm_lattice* lat, int rows, int planes) {
   CompactState& c = lat->compact;
   const int old_rows = c.rows, old_planes = c.planes;
@@ -238,8 +258,8 @@ mlbm_status compact_set_shape(mlbm_lattice* lat, int rows, int planes) {
 mlbm_status compact_enter(mlbm_lattice* lat) {
   CompactState& c = lat->compact;
   if (c.active) return MLBM_OK;
-  if (!c.supported)
-    return set_error(MLBM_ERR_ARG, "compact step does not support this lattice");
+  if (!c.supported && !c.two_pass_ok)
+    return set_error(MLBM_ERR_ARG, "compact layout does not support this lattice");
   if (!c.built)
     if (mlbm_status st = build_tables(lat)) return st;
   mlbm_status st;
@@ -249,6 +269,7 @@ mlbm_status compact_enter(mlbm_lattice* lat) {
   }
   if (st) return st;
   c.active = true;
+  c.parts_valid = true;
   return MLBM_OK;
 }
 
@@ -276,6 +297,8 @@ void compact_free(mlbm_lattice* lat) {
   CompactState& c = lat->compact;
   cudaFree(c.cpop);
   cudaFree(c.part);
+  cudaFree(c.cnb);
+  cudaFree(c.cinfo);
   cudaFree(c.wbase);
   cudaFree(c.tabs);
   c = CompactState{};
@@ -311,7 +334,7 @@ mlbm_status launch_compact(mlbm_lattice* lat, const StepArgs& a, int out) {
   CArgs cc = args_of(lat);
   void* args[] = {&cpop, &cc, &rho, &psi, &vel, &g, &p, &aa};
   cudaError_t e = cudaLaunchKernel(pick_step<T>(lat->phase, out),
-                                   dim3(c.nty * c.nzc), dim3(kThreads), args,
+                                   dim3(c.nty * c.nzc), dim3(kCompactThreads), args,
                                    c.smem, lat->stream);
   if (e != cudaSuccess) return cuda_fail(e, "compact time-step launch");
   return MLBM_OK;
@@ -319,5 +342,48 @@ mlbm_status launch_compact(mlbm_lattice* lat, const StepArgs& a, int out) {
 
 template mlbm_status launch_compact<float>(mlbm_lattice*, const StepArgs&, int);
 template mlbm_status launch_compact<__half>(mlbm_lattice*, const StepArgs&, int);
+
+namespace {
+template <typename T, int PHASE>
+void launch_c2(mlbm_lattice* lat, const StepArgs& a, bool wu, bool wr, bool inj) {
+  const CompactState& c = lat->compact;
+  const CArgs ca = args_of(lat);
+  const unsigned grid = (unsigned)((c.nfluid + kC2Threads - 1) / kC2Threads);
+  if (grid == 0) return;
+  T* cpop = static_cast<T*>(c.cpop);
+  float* rho = static_cast<float*>(lat->rho);
+  float* psi = static_cast<float*>(lat->psi);
+  if (wr)
+    k_cdensity<T, PHASE, true><<<grid, kC2Threads, 0, lat->stream>>>(
+        cpop, ca, c.cinfo, c.nfluid, rho, psi, lat->g, lat->phys, a, inj);
+  else
+    k_cdensity<T, PHASE, false><<<grid, kC2Threads, 0, lat->stream>>>(
+        cpop, ca, c.cinfo, c.nfluid, rho, psi, lat->g, lat->phys, a, inj);
+  if (wu)
+    k_cupdate<T, PHASE, true><<<grid, kC2Threads, 0, lat->stream>>>(
+        cpop, ca, c.cinfo, c.nfluid, psi, lat->vel, lat->g, lat->phys, a, inj);
+  else
+    k_cupdate<T, PHASE, false><<<grid, kC2Threads, 0, lat->stream>>>(
+        cpop, ca, c.cinfo, c.nfluid, psi, lat->vel, lat->g, lat->phys, a, inj);
+}
+}  // namespace
+
+template <typename T>
+mlbm_status launch_compact_two_pass(mlbm_lattice* lat, const StepArgs& a,
+                                    bool write_u, bool write_rho) {
+  const Phys& p = lat->phys;
+  const bool inj = p.rho_inject_period != 0ull &&
+                   (unsigned long long)a.step % p.rho_inject_period == 0ull;
+  if (lat->phase == 0)
+    launch_c2<T, 0>(lat, a, write_u, write_rho, inj);
+  else
+    launch_c2<T, 1>(lat, a, write_u, write_rho, inj);
+  const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(e, "compact two-pass launch");
+  return MLBM_OK;
+}
+
+template mlbm_status launch_compact_two_pass<float>(mlbm_lattice*, const StepArgs&, bool, bool);
+template mlbm_status launch_compact_two_pass<__half>(mlbm_lattice*, const StepArgs&, bool, bool);
 
 }  // namespace mlbm

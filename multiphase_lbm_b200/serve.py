@@ -159,10 +159,11 @@ def serve_batched(reqs, hbm_cap=150e9, chunk=CONVERGENCE_STEPS, log=None):
 
 
 def serve_fifo(reqs, chunk=CONVERGENCE_STEPS, log=None,
-               kernel=capi.KERNEL_TWO_PASS):
+               kernel=capi.KERNEL_AUTO):
     """Requests one at a time in arrival order, each alone on the GPU, with
-    the batch's two-pass kernels by default (then every result equals the
-    batched one bit for bit)."""
+    the fastest plain kernels (AUTO: the compact two-pass step, bit-identical
+    to the batch's kernels, so every result equals the batched one bit for
+    bit)."""
     t0 = time.perf_counter()
     for r in sorted(reqs, key=lambda q: q.arrival):
         now = time.perf_counter() - t0
@@ -207,8 +208,8 @@ def main(argv=None) -> int:
     ap.add_argument("--hbm-cap-gb", type=float, default=150.0)
     ap.add_argument("--seed", type=int, default=7)
     ap.add_argument("--no-fifo", action="store_true")
-    ap.add_argument("--fifo-kernel", default="two-pass",
-                    choices=["two-pass", "compact"])
+    ap.add_argument("--fifo-kernel", default="auto",
+                    choices=["auto", "two-pass", "compact"])
     a = ap.parse_args(argv)
     log = lambda s: print(s, file=sys.stderr, flush=True)  # noqa: E731
     reqs = make_requests(a.requests, a.rate, a.seed, a.budget_scale)
@@ -219,8 +220,8 @@ def main(argv=None) -> int:
            "batched": summarise(mk, done)}
     if not a.no_fifo:
         reqs2 = make_requests(a.requests, a.rate, a.seed, a.budget_scale)
-        kern = (capi.KERNEL_TWO_PASS if a.fifo_kernel == "two-pass"
-                else capi.KERNEL_COMPACT)
+        kern = {"auto": capi.KERNEL_AUTO, "two-pass": capi.KERNEL_TWO_PASS,
+                "compact": capi.KERNEL_COMPACT}[a.fifo_kernel]
         mk2, done2 = serve_fifo(reqs2, log=log, kernel=kern)
         out["fifo_kernel"] = a.fifo_kernel
         out["fifo"] = summarise(mk2, done2)

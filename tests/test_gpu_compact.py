@@ -1,11 +1,13 @@
-"""The single-pass step over the compact (fluid-only) layout.
+"""The kernels over the compact (fluid-only) population layout.
 
-Its collision is the two-pass collision; psi of the next step is formed from
-fixed-point part sums of the post-collision populations instead of a second
-pass, so it agrees with the reference's kernels (the oracle) to rounding.
-Tolerances (the FP32 parity bar): density within 1e-5 relative pointwise,
-populations and velocity within 1e-5 relative to their largest value, over
-the first 100 steps; FP16 storage: density within 2e-3 relative.
+COMPACT runs the two passes of the dense kernels over the compact layout and
+must match them bit for bit.  SINGLE_PASS has the same collision but forms
+psi of the next step from fixed-point part sums of the post-collision
+populations instead of a second pass, so it agrees with the reference's
+kernels (the oracle) to rounding.  Tolerances (the FP32 parity bar): density
+within 1e-5 relative pointwise, populations and velocity within 1e-5 relative
+to their largest value, over the first 100 steps; FP16 storage: density
+within 2e-3 relative.
 """
 import numpy as np
 import pytest
@@ -30,12 +32,16 @@ def _lattice(capi, shape, fluid, rho, kernel, storage=0, shape_kc=None, **kw):
     return lat
 
 
-def test_compact_matches_oracle_drainage_100_steps():
+KINDS = [3, 4]  # KERNEL_COMPACT, KERNEL_SINGLE_PASS
+
+
+@pytest.mark.parametrize("kind", KINDS)
+def test_compact_matches_oracle_drainage_100_steps(kind):
     from multiphase_lbm_b200 import capi
     shape = (64, 48, 40)
     fluid, rho = sphere_case(shape, seed=11, rmin=3.0, rmax=6.0, porosity=0.55,
                              rho0=1.9, amp=0.02)
-    lat = _lattice(capi, shape, fluid, rho, capi.KERNEL_COMPACT, **DRAIN)
+    lat = _lattice(capi, shape, fluid, rho, kind, **DRAIN)
     port = oracle.Port(rho, fluid, oracle.make_params(**DRAIN))
     m = fluid.astype(bool)
     step = 0
@@ -60,12 +66,13 @@ CASES = [((40, 32, 24), (4, 8)), ((33, 5, 7), (2, 2)), ((70, 9, 4), (4, 2)),
 
 
 @pytest.mark.parametrize("shape,kc", CASES)
-def test_compact_agrees_with_two_pass(shape, kc):
+def test_single_pass_agrees_with_two_pass(shape, kc):
     from multiphase_lbm_b200 import capi
     fluid, rho = sphere_case(shape, seed=sum(shape), rmin=1.5, rmax=3.5,
                              porosity=0.6, rho0=0.7, amp=0.1)
     kw = dict(G=-5.0, rhos=0.223144, tau=1.0)
-    a = _lattice(capi, shape, fluid, rho, capi.KERNEL_COMPACT, shape_kc=kc, **kw)
+    a = _lattice(capi, shape, fluid, rho, capi.KERNEL_SINGLE_PASS, shape_kc=kc,
+                 **kw)
     b = _lattice(capi, shape, fluid, rho, capi.KERNEL_TWO_PASS, **kw)
     m = fluid.astype(bool)
     for s0, n in ((0, 1), (1, 2), (3, 47)):
@@ -77,13 +84,36 @@ def test_compact_agrees_with_two_pass(shape, kc):
         assert e <= 1e-5, f"{shape} {kc} step {s0 + n}: populations {e:.3e}"
 
 
-def test_compact_fp16_close_to_two_pass_fp16():
+@pytest.mark.parametrize("storage", [0, 1])
+@pytest.mark.parametrize("shape", [(40, 32, 24), (33, 5, 7), (70, 3, 2),
+                                   (300, 6, 6), (1, 9, 8)])
+def test_compact_two_pass_bit_identical(shape, storage):
+    """Same loads, same arithmetic: the compact two-pass step equals the
+    dense two-pass step bit for bit (drainage slabs, velocity output)."""
+    from multiphase_lbm_b200 import capi
+    fluid, rho = sphere_case(shape, seed=sum(shape) + storage, rmin=1.5,
+                             rmax=3.5, porosity=0.6, rho0=1.5, amp=0.3)
+    kw = dict(G=-5.0, rhos=0.223144, tau=1.0, rho_shift=1.0)
+    if shape[0] >= 8:
+        kw.update(inlet_width=2, outlet_width=1, rho_inlet=0.17, rho_outlet=1.9)
+    outs = []
+    for kind in (capi.KERNEL_COMPACT, capi.KERNEL_TWO_PASS):
+        lat = _lattice(capi, shape, fluid, rho, kind, storage=storage, **kw)
+        lat.iterate(0, 20)
+        lat.iterate(20, 1, write_velocity=True)
+        outs.append((lat.field("rho"), lat.field("f"), lat.field("velocity"),
+                     lat.field("psi")))
+    for u, v in zip(*outs):
+        assert np.array_equal(u, v)
+
+
+def test_single_pass_fp16_close_to_two_pass_fp16():
     from multiphase_lbm_b200 import capi
     shape = (48, 40, 32)
     fluid, rho = sphere_case(shape, seed=4, rmin=2.0, rmax=5.0, porosity=0.55,
                              rho0=1.9, amp=0.02)
     kw = dict(DRAIN, rho_shift=1.0)
-    a = _lattice(capi, shape, fluid, rho, capi.KERNEL_COMPACT,
+    a = _lattice(capi, shape, fluid, rho, capi.KERNEL_SINGLE_PASS,
                  storage=capi.STORE_F16, **kw)
     b = _lattice(capi, shape, fluid, rho, capi.KERNEL_TWO_PASS,
                  storage=capi.STORE_F16, **kw)
@@ -94,14 +124,14 @@ def test_compact_fp16_close_to_two_pass_fp16():
     assert e <= 2e-3, f"fp16 rho {e:.3e}"
 
 
-def test_compact_deterministic_bitwise():
+def test_single_pass_deterministic_bitwise():
     from multiphase_lbm_b200 import capi
     shape = (64, 32, 32)
     fluid, rho = sphere_case(shape, seed=9, rmin=2.0, rmax=5.0, porosity=0.5,
                              rho0=0.7, amp=0.05)
     outs = []
     for _ in range(2):
-        lat = _lattice(capi, shape, fluid, rho, capi.KERNEL_AUTO,
+        lat = _lattice(capi, shape, fluid, rho, capi.KERNEL_SINGLE_PASS,
                        G=-6.0, rhos=0.182322)
         lat.iterate(0, 60)
         outs.append((lat.field("rho"), lat.field("f")))
@@ -110,16 +140,18 @@ def test_compact_deterministic_bitwise():
 
 
 def test_kernel_switching_keeps_the_state():
-    """compact -> two-pass -> compact, against two-pass throughout."""
+    """single-pass -> two-pass -> compact -> single-pass -> fused, against
+    two-pass throughout."""
     from multiphase_lbm_b200 import capi
     shape = (40, 24, 20)
     fluid, rho = sphere_case(shape, seed=2, rmin=2.0, rmax=4.0, porosity=0.6,
                              rho0=1.9, amp=0.02)
-    a = _lattice(capi, shape, fluid, rho, capi.KERNEL_COMPACT, **DRAIN)
+    a = _lattice(capi, shape, fluid, rho, capi.KERNEL_SINGLE_PASS, **DRAIN)
     b = _lattice(capi, shape, fluid, rho, capi.KERNEL_TWO_PASS, **DRAIN)
     step = 0
-    for kind in (capi.KERNEL_COMPACT, capi.KERNEL_TWO_PASS,
-                 capi.KERNEL_COMPACT, capi.KERNEL_FUSED):
+    for kind in (capi.KERNEL_SINGLE_PASS, capi.KERNEL_TWO_PASS,
+                 capi.KERNEL_COMPACT, capi.KERNEL_SINGLE_PASS,
+                 capi.KERNEL_FUSED):
         a.set_step_kernel(kind)
         a.iterate(step, 15)
         b.iterate(step, 15)
@@ -129,12 +161,12 @@ def test_kernel_switching_keeps_the_state():
     assert rel_err(a.field("f"), b.field("f"), m) <= 1e-5
 
 
-def test_compact_shape_and_autotune():
+def test_single_pass_shape_and_autotune():
     from multiphase_lbm_b200 import capi
     shape = (64, 32, 32)
     fluid, rho = sphere_case(shape, seed=5, rmin=2.0, rmax=5.0, porosity=0.5,
                              rho0=1.9, amp=0.02)
-    a = _lattice(capi, shape, fluid, rho, capi.KERNEL_COMPACT, **DRAIN)
+    a = _lattice(capi, shape, fluid, rho, capi.KERNEL_SINGLE_PASS, **DRAIN)
     b = _lattice(capi, shape, fluid, rho, capi.KERNEL_TWO_PASS, **DRAIN)
     rows, planes, done = a.autotune(0, trial_steps=2)
     assert 2 <= rows <= 8 and 2 <= planes <= 32 and done > 0
@@ -148,11 +180,15 @@ def test_compact_shape_and_autotune():
         a.set_compact_shape(1, 8)      # tiles need two rows at least
 
 
-def test_compact_rejects_fp64_and_flat_lattices():
+def test_compact_kernels_reject_what_they_cannot_run():
     from multiphase_lbm_b200 import capi
     lat = capi.Lattice((16, 16, 16), storage=capi.STORE_F64)
-    with pytest.raises(capi.MlbmError):
-        lat.set_step_kernel(capi.KERNEL_COMPACT)
+    for kind in (capi.KERNEL_COMPACT, capi.KERNEL_SINGLE_PASS):
+        with pytest.raises(capi.MlbmError):
+            lat.set_step_kernel(kind)
+    assert lat.step_kernel == capi.KERNEL_TWO_PASS       # AUTO on FP64
     lat = capi.Lattice((16, 3, 16))
     with pytest.raises(capi.MlbmError):
-        lat.set_step_kernel(capi.KERNEL_COMPACT)
+        lat.set_step_kernel(capi.KERNEL_SINGLE_PASS)     # needs ly >= 4
+    lat.set_step_kernel(capi.KERNEL_COMPACT)
+    assert capi.Lattice((16, 16, 16)).step_kernel == capi.KERNEL_COMPACT
