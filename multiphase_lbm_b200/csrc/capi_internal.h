@@ -31,6 +31,7 @@ struct CompactState {
   float* part = nullptr;       // [2][4][cs] part sums of rho (two sets)
   uint32_t* cnb = nullptr;     // [cs] neighbour words in compact order
   uint2* cinfo = nullptr;      // [cs] (neighbour word, packed x, y, z)
+  uint2* wtab = nullptr;       // [rows * wpr + 1] (mask word, wbase)
   bool two_pass_ok = false;    // the compact two-pass kernels fit the lattice
   uint32_t* wbase = nullptr;   // [rows * wpr + 1]
   int* tabs = nullptr;         // ytab[ly], ztab[lz], ystart[nty+1], zstart[nzc+1]

@@ -118,6 +118,12 @@ mlbm_status build_tables(mlbm_lattice* lat) {
   e = cudaMemcpy(c.wbase, h.data(), (nwords + 1) * sizeof(uint32_t),
                  cudaMemcpyHostToDevice);
   if (e != cudaSuccess) return cuda_fail(e, "compact tables");
+  if (c.wtab) cudaFree(c.wtab);
+  c.wtab = nullptr;
+  e = cudaMalloc((void**)&c.wtab, (nwords + 1) * sizeof(uint2));
+  if (e != cudaSuccess) return cuda_fail(e, "compact tables");
+  k_wtab<<<(unsigned)((nwords + 256) / 256), 256, 0, lat->stream>>>(
+      lat->mask, c.wbase, c.wtab, nwords);
   c.nfluid = (long long)run;
   c.cs = std::max(64LL, (c.nfluid + 63) / 64 * 64);
   if (c.cs > c.cap) {
@@ -300,6 +306,7 @@ void compact_free(mlbm_lattice* lat) {
   cudaFree(c.cnb);
   cudaFree(c.cinfo);
   cudaFree(c.wbase);
+  cudaFree(c.wtab);
   cudaFree(c.tabs);
   c = CompactState{};
 }
@@ -355,16 +362,16 @@ void launch_c2(mlbm_lattice* lat, const StepArgs& a, bool wu, bool wr, bool inj)
   float* psi = static_cast<float*>(lat->psi);
   if (wr)
     k_cdensity<T, PHASE, true><<<grid, kC2Threads, 0, lat->stream>>>(
-        cpop, ca, c.cinfo, c.nfluid, rho, psi, lat->g, lat->phys, a, inj);
+        cpop, ca, c.cinfo, c.wtab, c.nfluid, rho, psi, lat->g, lat->phys, a, inj);
   else
     k_cdensity<T, PHASE, false><<<grid, kC2Threads, 0, lat->stream>>>(
-        cpop, ca, c.cinfo, c.nfluid, rho, psi, lat->g, lat->phys, a, inj);
+        cpop, ca, c.cinfo, c.wtab, c.nfluid, rho, psi, lat->g, lat->phys, a, inj);
   if (wu)
     k_cupdate<T, PHASE, true><<<grid, kC2Threads, 0, lat->stream>>>(
-        cpop, ca, c.cinfo, c.nfluid, psi, lat->vel, lat->g, lat->phys, a, inj);
+        cpop, ca, c.cinfo, c.wtab, c.nfluid, psi, lat->vel, lat->g, lat->phys, a, inj);
   else
     k_cupdate<T, PHASE, false><<<grid, kC2Threads, 0, lat->stream>>>(
-        cpop, ca, c.cinfo, c.nfluid, psi, lat->vel, lat->g, lat->phys, a, inj);
+        cpop, ca, c.cinfo, c.wtab, c.nfluid, psi, lat->vel, lat->g, lat->phys, a, inj);
 }
 }  // namespace
 

@@ -45,41 +45,53 @@ static __global__ void k_cinfo(const uint32_t* __restrict__ nbw,
 
 // Compact indices of the 18 neighbours x + e_i of fluid node k at (x, y, z)
 // (meaningful where the neighbour is fluid): the rank of x in each
-// neighbour row from the global tables, then x - 1 -> rank - 1 and x + 1 ->
-// rank + fluid(x), with the periodic wrap in x.
-__device__ __forceinline__ void neighbour_ranks(const CArgs& c, const Geom& g,
-                                                int k, int x, int y, int z,
-                                                int (&nk)[Q]) {
+// neighbour row from wtab[word] = (mask word, wbase), then x - 1 -> rank - 1
+// and x + 1 -> rank + fluid(x), with the periodic wrap in x (row start =
+// wtab[first word].y, row end = wtab[first word + wpr].y, the next row's
+// start; wtab has one sentinel entry after the last row).  32-bit indices:
+// the table has fewer than 2^31 words.
+__device__ __forceinline__ void neighbour_ranks(const uint2* __restrict__ wtab,
+                                                const Geom& g, int k, int x,
+                                                int y, int z, int (&nk)[Q]) {
   const int ym = y == 0 ? g.ly - 1 : y - 1, yp = y == g.ly - 1 ? 0 : y + 1;
   const int zm = z == 0 ? g.lz - 1 : z - 1, zp = z == g.lz - 1 ? 0 : z + 1;
   const bool xlo = x == 0, xhi = x == g.lx - 1;
-  const int w = x >> 5;
+  const int w = x >> 5, xb = x & 31;
   const uint32_t lb = low_bits(x);
   const int wpr = g.wpr;
-  auto rank3 = [&](int yy, int zz, int& r_, int& rl, int& rh) {
-    const long long r = ((long long)zz * g.ly + yy) * wpr;
-    const uint32_t m = __ldg(c.mask + r + w);
-    r_ = (int)__ldg(c.wbase + r + w) + __popc(m & lb);
-    rl = xlo ? (int)__ldg(c.wbase + r + wpr) - 1 : r_ - 1;
-    rh = xhi ? (int)__ldg(c.wbase + r) : r_ + (int)((m >> (x & 31)) & 1u);
+  const int pz = z * g.ly, pzm = zm * g.ly, pzp = zp * g.ly;
+  auto rank3 = [&](int row, int& r_, int& rl, int& rh) {
+    const int rb = row * wpr;
+    const uint2 v = __ldg(wtab + rb + w);
+    r_ = (int)v.y + __popc(v.x & lb);
+    rl = xlo ? (int)__ldg(wtab + rb + wpr).y - 1 : r_ - 1;
+    rh = xhi ? (int)__ldg(wtab + rb).y : r_ + (int)((v.x >> xb) & 1u);
   };
-  auto rank1 = [&](int yy, int zz) {
-    const long long r = ((long long)zz * g.ly + yy) * wpr;
-    return (int)__ldg(c.wbase + r + w) + __popc(__ldg(c.mask + r + w) & lb);
+  auto rank1 = [&](int row) {
+    const uint2 v = __ldg(wtab + row * wpr + w);
+    return (int)v.y + __popc(v.x & lb);
   };
-  const long long r0 = ((long long)z * g.ly + y) * wpr;
+  const int r0 = (pz + y) * wpr;
   nk[0] = k;
-  nk[1] = xlo ? (int)__ldg(c.wbase + r0 + wpr) - 1 : k - 1;  // (-1, 0, 0)
-  nk[10] = xhi ? (int)__ldg(c.wbase + r0) : k + 1;           // (+1, 0, 0)
+  nk[1] = xlo ? (int)__ldg(wtab + r0 + wpr).y - 1 : k - 1;  // (-1, 0, 0)
+  nk[10] = xhi ? (int)__ldg(wtab + r0).y : k + 1;           // (+1, 0, 0)
   int r_, rl, rh;
-  rank3(ym, z, r_, rl, rh);  nk[2] = r_;  nk[4] = rl; nk[14] = rh;
-  rank3(yp, z, r_, rl, rh);  nk[11] = r_; nk[5] = rl; nk[13] = rh;
-  rank3(y, zm, r_, rl, rh);  nk[3] = r_;  nk[6] = rl; nk[16] = rh;
-  rank3(y, zp, r_, rl, rh);  nk[12] = r_; nk[7] = rl; nk[15] = rh;
-  nk[8] = rank1(ym, zm);   // (0, -1, -1)
-  nk[9] = rank1(ym, zp);   // (0, -1, +1)
-  nk[17] = rank1(yp, zp);  // (0, +1, +1)
-  nk[18] = rank1(yp, zm);  // (0, +1, -1)
+  rank3(pz + ym, r_, rl, rh);  nk[2] = r_;  nk[4] = rl; nk[14] = rh;
+  rank3(pz + yp, r_, rl, rh);  nk[11] = r_; nk[5] = rl; nk[13] = rh;
+  rank3(pzm + y, r_, rl, rh);  nk[3] = r_;  nk[6] = rl; nk[16] = rh;
+  rank3(pzp + y, r_, rl, rh);  nk[12] = r_; nk[7] = rl; nk[15] = rh;
+  nk[8] = rank1(pzm + ym);   // (0, -1, -1)
+  nk[9] = rank1(pzp + ym);   // (0, -1, +1)
+  nk[17] = rank1(pzp + yp);  // (0, +1, +1)
+  nk[18] = rank1(pzm + yp);  // (0, +1, -1)
+}
+
+// wtab[i] = (mask word i, wbase[i]); wtab[nwords] = (0, fluid node count).
+static __global__ void k_wtab(const uint32_t* __restrict__ mask,
+                              const uint32_t* __restrict__ wbase,
+                              uint2* __restrict__ wtab, long long nwords) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i <= nwords) wtab[i] = make_uint2(i < nwords ? mask[i] : 0u, wbase[i]);
 }
 
 template <typename T, int PHASE>
@@ -101,7 +113,8 @@ __device__ __forceinline__ void cgather(const T* __restrict__ cpop, long long cs
 template <typename T, int PHASE, bool WRITE_RHO>
 __global__ void __launch_bounds__(kC2Threads)
     k_cdensity(const T* __restrict__ cpop, CArgs c,
-               const uint2* __restrict__ cinfo, long long nfluid,
+               const uint2* __restrict__ cinfo, const uint2* __restrict__ wtab,
+               long long nfluid,
                float* __restrict__ rho_out, float* __restrict__ psi, Geom g,
                Phys p, StepArgs a, bool inj) {
   const long long kk = (long long)blockIdx.x * kC2Threads + threadIdx.x;
@@ -117,7 +130,7 @@ __global__ void __launch_bounds__(kC2Threads)
     d = slab_density(p, kind);
   } else {
     int nk[Q];
-    if (PHASE == 0) neighbour_ranks(c, g, k, x, y, z, nk);
+    if (PHASE == 0) neighbour_ranks(wtab, g, k, x, y, z, nk);
     float f[Q];
     cgather<T, PHASE>(cpop, c.cs, k, nb, nk, p.rho_shift, f);
     d = 0.f;
@@ -132,7 +145,8 @@ __global__ void __launch_bounds__(kC2Threads)
 template <typename T, int PHASE, bool WRITE_U>
 __global__ void __launch_bounds__(kC2Threads)
     k_cupdate(T* __restrict__ cpop, CArgs c, const uint2* __restrict__ cinfo,
-              long long nfluid, const float* __restrict__ psi,
+              const uint2* __restrict__ wtab, long long nfluid,
+              const float* __restrict__ psi,
               float* __restrict__ vel, Geom g, Phys p, StepArgs a, bool inj) {
   const long long kk = (long long)blockIdx.x * kC2Threads + threadIdx.x;
   if (kk >= nfluid) return;
@@ -144,7 +158,7 @@ __global__ void __launch_bounds__(kC2Threads)
   const int kind = nb_kind(nb);
   const float shift = p.rho_shift;
   int nk[Q];
-  if (PHASE == 0) neighbour_ranks(c, g, k, x, y, z, nk);
+  if (PHASE == 0) neighbour_ranks(wtab, g, k, x, y, z, nk);
   float f[Q];
   float ux = 0.f, uy = 0.f, uz = 0.f;
   if (kind) {
