@@ -81,7 +81,8 @@ def load_traffic(kernel, storage):
 
 
 # roofline label and launches per step of each step kernel
-KERNEL_INFO = {4: ("single-pass", "k_compact_step (single pass, compact layout)", 1),
+KERNEL_INFO = {5: ("wave", "k_cwave (wavefront step, compact layout)", 1),
+               4: ("single-pass", "k_compact_step (single pass, compact layout)", 1),
                3: ("compact", "time step (k_cdensity + k_cupdate, compact layout)", 2),
                2: ("two-pass", "time step (k_density + k_update_zm)", 2),
                1: ("fused", "k_step_fused (persistent)", 1)}
@@ -221,7 +222,10 @@ def main():
     ap.add_argument("--size", type=int, default=200,
                     help="lattice edge (profiling runs use a smaller case)")
     ap.add_argument("--kernel", default="auto",
-                    choices=["auto", "compact", "single-pass", "fused", "two-pass"])
+                    choices=["auto", "wave", "compact", "single-pass", "fused",
+                             "two-pass"])
+    ap.add_argument("--wave-shape", default=None,
+                    help="tile_nodes,lookahead of the wavefront step")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -251,11 +255,14 @@ def main():
     lat.set_params(params)
     lat.upload(fluid, rho)
     lat.initialize()
-    kernel_id = {"auto": capi.KERNEL_AUTO, "compact": capi.KERNEL_COMPACT,
+    kernel_id = {"auto": capi.KERNEL_AUTO, "wave": capi.KERNEL_WAVE,
+                 "compact": capi.KERNEL_COMPACT,
                  "single-pass": capi.KERNEL_SINGLE_PASS,
                  "fused": capi.KERNEL_FUSED,
                  "two-pass": capi.KERNEL_TWO_PASS}[args.kernel]
     lat.set_step_kernel(kernel_id)
+    if args.wave_shape:
+        lat.set_wave_shape(*[int(v) for v in args.wave_shape.split(",")])
     kname, klabel, klaunches = KERNEL_INFO[lat.step_kernel]
     step = 0
     lat.iterate(step, args.warmup)

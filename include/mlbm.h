@@ -188,6 +188,11 @@ mlbm_status mlbm_iterate(mlbm_lattice* lat, int64_t step0, int32_t nsteps,
  *                formed from a differently ordered sum of the same
  *                populations, so results agree with TWO_PASS to rounding (not
  *                bit for bit) and are deterministic;
+ *   WAVE         the two passes over the fluid-only layout in ONE persistent
+ *                launch per step: density tiles run a few planes ahead of
+ *                the update tiles (a wavefront along z), so the update reads
+ *                the populations back from L2 and DRAM sees them once per
+ *                step.  Bit-identical to TWO_PASS; same limits as COMPACT;
  *   AUTO         (default) COMPACT where supported, else TWO_PASS.
  * The state moves between the layouts on demand (the dense buffers stay
  * allocated; the fluid-only layout adds 19 populations and 14 words per
@@ -197,9 +202,15 @@ mlbm_status mlbm_iterate(mlbm_lattice* lat, int64_t step0, int32_t nsteps,
 #define MLBM_KERNEL_TWO_PASS 2
 #define MLBM_KERNEL_COMPACT 3
 #define MLBM_KERNEL_SINGLE_PASS 4
+#define MLBM_KERNEL_WAVE 5
 mlbm_status mlbm_set_step_kernel(mlbm_lattice* lat, int32_t kind);
 /* The kernel the next mlbm_iterate runs (AUTO resolved); -1 for NULL. */
 int32_t mlbm_get_step_kernel(const mlbm_lattice* lat);
+/* Work items of the WAVE step: `tile_nodes` fluid nodes per item (32..65536,
+ * default 1024) and the lead of the density tiles over the update tiles in
+ * planes (0..256, default 4). */
+mlbm_status mlbm_set_wave_shape(mlbm_lattice* lat, int32_t tile_nodes,
+                                int32_t lookahead);
 /* Tiling of the SINGLE_PASS step: a block walks `rows` full x-rows (y) through
  * `planes` planes (z); at least two tiles along y and z, each at least two
  * rows / planes deep.  Default 4 x 8. */
@@ -215,16 +226,16 @@ mlbm_status mlbm_set_tuning(mlbm_lattice* lat, int32_t rows_per_item,
 mlbm_status mlbm_set_update_shape(mlbm_lattice* lat, int32_t rows,
                                   int32_t planes);
 /* Time candidate shapes of the lattice's step kernel (update shape for
- * TWO_PASS, tiling for SINGLE_PASS; COMPACT has none: out = {0, 0}, no
- * steps) and keep the fastest.  The trial steps are
+ * TWO_PASS, tiling for SINGLE_PASS, tile nodes x lookahead for WAVE; COMPACT
+ * has none: out = {0, 0}, no steps) and keep the fastest.  The trial steps are
  * real steps (step0, step0+1, ...): the lattice advances by *steps_done of
  * them.  out (optional, 2 ints) receives rows, planes. */
 mlbm_status mlbm_autotune(mlbm_lattice* lat, int64_t step0,
                           int32_t trial_steps, int32_t* out,
                           int32_t* steps_done);
 /* Wait for the lattice's stream and report a device-side failure (a bounded
- * wait of the fused kernel that ran out: MLBM_ERR_TIMEOUT; the lattice must
- * then be initialised again). */
+ * wait of the fused or wavefront kernel that ran out: MLBM_ERR_TIMEOUT; the
+ * lattice must then be initialised again). */
 mlbm_status mlbm_synchronize(mlbm_lattice* lat);
 
 /* Copy a field out in the reference layout.  dtype: MLBM_DTYPE_F32 or

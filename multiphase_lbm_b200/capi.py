@@ -20,8 +20,8 @@ FIELD_RHO, FIELD_PRESSURE, FIELD_PSI, FIELD_VELOCITY, FIELD_POPULATIONS, \
     FIELD_FLUID = range(6)
 DTYPE_F32, DTYPE_F64, DTYPE_U8 = 0, 1, 2
 ITER_WRITE_VELOCITY = 1
-KERNEL_AUTO, KERNEL_FUSED, KERNEL_TWO_PASS, KERNEL_COMPACT, KERNEL_SINGLE_PASS = \
-    0, 1, 2, 3, 4
+(KERNEL_AUTO, KERNEL_FUSED, KERNEL_TWO_PASS, KERNEL_COMPACT,
+ KERNEL_SINGLE_PASS, KERNEL_WAVE) = 0, 1, 2, 3, 4, 5
 Q = 19
 
 STATUS = {0: "MLBM_OK", 1: "MLBM_ERR_ARG", 2: "MLBM_ERR_CUDA",
@@ -114,6 +114,7 @@ SIGNATURES = [
     ("mlbm_synchronize", C.c_int, [_VP]),
     ("mlbm_set_update_shape", C.c_int, [_VP, C.c_int32, C.c_int32]),
     ("mlbm_set_compact_shape", C.c_int, [_VP, C.c_int32, C.c_int32]),
+    ("mlbm_set_wave_shape", C.c_int, [_VP, C.c_int32, C.c_int32]),
     ("mlbm_get_step_kernel", C.c_int32, [_VP]),
     ("mlbm_autotune", C.c_int, [_VP, C.c_int64, C.c_int32, _VP, _VP]),
     ("mlbm_phase_stats_noalloc", C.c_int, [_VP, _VP, C.c_int32, C.c_int32,
@@ -195,6 +196,11 @@ class Lattice:
         """The kernel the next iterate runs (KERNEL_COMPACT, ... ; AUTO
         resolved)."""
         return int(lib().mlbm_get_step_kernel(self.h))
+
+    def set_wave_shape(self, tile_nodes: int = 1024, lookahead: int = 4) -> None:
+        """Work items of the wavefront step: fluid nodes per item and the
+        lead of the density tiles over the update tiles, in planes."""
+        check(lib().mlbm_set_wave_shape(self.h, tile_nodes, lookahead))
 
     def set_compact_shape(self, rows: int = 4, planes: int = 8) -> None:
         """Tiling of the single-pass step (rows along y, planes along z)."""

@@ -205,8 +205,8 @@ mlbm_status launch_two_pass(mlbm_lattice* lat, const StepArgs& a, bool wu,
 // One lattice step per launch (two launches for the two-pass kernels, which
 // AUTO selects).  rho is written on the last step of each mlbm_iterate call
 // (the field the caller can read afterwards).
-// The step kernel a lattice runs: AUTO is the compact single-pass step where
-// it supports the lattice (FP32 / FP16 storage), else the two-pass step.
+// The step kernel a lattice runs: AUTO is the compact two-pass step where it
+// supports the lattice (FP32 / FP16 storage), else the dense two-pass step.
 int effective_kernel(const mlbm_lattice* lat) {
   if (lat->step_kernel != MLBM_KERNEL_AUTO) return lat->step_kernel;
   return lat->compact.two_pass_ok ? MLBM_KERNEL_COMPACT : MLBM_KERNEL_TWO_PASS;
@@ -220,10 +220,12 @@ mlbm_status launch_steps(mlbm_lattice* lat, int64_t step0, int32_t nsteps,
   const bool fused = kind == MLBM_KERNEL_FUSED && lat->fused.ok;
   if (kind == MLBM_KERNEL_FUSED && !lat->fused.ok)
     return fail(MLBM_ERR_ARG, "fused kernel does not fit this lattice");
-  bool compact = false, single = false;
+  bool compact = false, single = false, wave = false;
   if constexpr (!std::is_same<T, double>::value) {
-    compact = kind == MLBM_KERNEL_COMPACT || kind == MLBM_KERNEL_SINGLE_PASS;
+    compact = kind == MLBM_KERNEL_COMPACT || kind == MLBM_KERNEL_SINGLE_PASS ||
+              kind == MLBM_KERNEL_WAVE;
     single = kind == MLBM_KERNEL_SINGLE_PASS;
+    wave = kind == MLBM_KERNEL_WAVE;
   }
   if ((flags & MLBM_ITER_WRITE_VELOCITY) && !lat->vel) {
     // the velocity field is allocated on first request
@@ -251,6 +253,7 @@ mlbm_status launch_steps(mlbm_lattice* lat, int64_t step0, int32_t nsteps,
     mlbm_status st;
     if constexpr (!std::is_same<T, double>::value) {
       if (single) st = launch_compact<T>(lat, a, out);
+      else if (wave) st = launch_compact_wave<T>(lat, a, wu, last);
       else if (compact) st = launch_compact_two_pass<T>(lat, a, wu, last);
       else if (fused) st = launch_fused<T>(lat, a, out);
       else st = launch_two_pass<T>(lat, a, wu, last);
@@ -343,10 +346,11 @@ mlbm_status check_device_error(mlbm_lattice* lat) {
   cudaMemset(lat->err, 0, sizeof(int));
   cudaMemset(lat->pdone, 0, sizeof(unsigned) * max_tiles(lat->g));
   lat->fused_epoch = 0;
+  compact_reset_wave(lat);
   lat->initialized = false;
   return fail(MLBM_ERR_TIMEOUT,
-              "a bounded wait of the fused time step ran out; the lattice "
-              "must be initialised again");
+              "a bounded wait of the time step (fused or wavefront kernel) ran "
+              "out; the lattice must be initialised again");
 }
 
 mlbm_status ensure_staging(mlbm_lattice* lat, size_t bytes) {
@@ -743,11 +747,12 @@ mlbm_status mlbm_plane_profile(mlbm_lattice* lat, int64_t* n_fluid_x,
 
 mlbm_status mlbm_set_step_kernel(mlbm_lattice* lat, int32_t kind) {
   if (mlbm_status st = check_lat(lat)) return st;
-  if (kind < MLBM_KERNEL_AUTO || kind > MLBM_KERNEL_SINGLE_PASS)
+  if (kind < MLBM_KERNEL_AUTO || kind > MLBM_KERNEL_WAVE)
     return fail(MLBM_ERR_ARG, "invalid step kernel %d", kind);
   if (kind == MLBM_KERNEL_FUSED && !lat->fused.ok)
     return fail(MLBM_ERR_ARG, "fused kernel does not fit this lattice");
-  if (kind == MLBM_KERNEL_COMPACT && !lat->compact.two_pass_ok)
+  if ((kind == MLBM_KERNEL_COMPACT || kind == MLBM_KERNEL_WAVE) &&
+      !lat->compact.two_pass_ok)
     return fail(MLBM_ERR_ARG,
                 "compact kernels need FP32 or FP16 storage and at most "
                 "2048 x 2048 x 1024 nodes");
@@ -789,6 +794,17 @@ int32_t mlbm_get_step_kernel(const mlbm_lattice* lat) {
   return lat ? effective_kernel(lat) : -1;
 }
 
+mlbm_status mlbm_set_wave_shape(mlbm_lattice* lat, int32_t tile_nodes,
+                                int32_t lookahead) {
+  if (mlbm_status st = check_lat(lat)) return st;
+  if (tile_nodes < 32 || tile_nodes > 65536 || lookahead < 0 || lookahead > 256)
+    return fail(MLBM_ERR_ARG, "invalid wavefront shape %d nodes, %d planes ahead",
+                tile_nodes, lookahead);
+  if (mlbm_status st = activate(lat)) return st;
+  CUDA_TRY(cudaStreamSynchronize(lat->stream), "wavefront shape");
+  return compact_set_wave_shape(lat, tile_nodes, lookahead);
+}
+
 mlbm_status mlbm_set_compact_shape(mlbm_lattice* lat, int32_t rows,
                                    int32_t planes) {
   if (mlbm_status st = check_lat(lat)) return st;
@@ -813,20 +829,29 @@ mlbm_status mlbm_autotune(mlbm_lattice* lat, int64_t step0,
     return MLBM_OK;
   }
   const bool compact = effective_kernel(lat) == MLBM_KERNEL_SINGLE_PASS;
+  const bool wave = effective_kernel(lat) == MLBM_KERNEL_WAVE;
   const int rows_u[] = {1, 2, 4, 8};
   const int planes_u[] = {2, 4, 8, 16, 32};
   const int rows_k[] = {2, 3, 4, 6, 8};
   const int planes_k[] = {4, 8, 16, 32};
-  const int* rows_c = compact ? rows_k : rows_u;
-  const int* planes_c = compact ? planes_k : planes_u;
-  const int nr = compact ? 5 : 4, np = compact ? 4 : 5;
+  // wavefront: nodes per work item x planes of lookahead
+  const int tile_w[] = {256, 512, 1024, 2048};
+  const int ahead_w[] = {1, 2, 4, 8, 16};
+  const int* rows_c = wave ? tile_w : compact ? rows_k : rows_u;
+  const int* planes_c = wave ? ahead_w : compact ? planes_k : planes_u;
+  const int nr = wave ? 4 : compact ? 5 : 4, np = wave ? 5 : compact ? 4 : 5;
   cudaEvent_t e0, e1;
   CUDA_TRY(cudaEventCreate(&e0), "autotune");
   CUDA_TRY(cudaEventCreate(&e1), "autotune");
   float best = 1e30f;
-  int br = compact ? lat->compact.rows : lat->zm.By;
-  int bp = compact ? lat->compact.planes : lat->zm.Dz;
+  int br = wave ? lat->compact.wave_tile : compact ? lat->compact.rows : lat->zm.By;
+  int bp = wave ? lat->compact.wave_lookahead
+                : compact ? lat->compact.planes : lat->zm.Dz;
   auto apply = [&](int r, int pl) -> mlbm_status {
+    if (wave) {
+      CUDA_TRY(cudaStreamSynchronize(lat->stream), "autotune");
+      return compact_set_wave_shape(lat, r, pl);
+    }
     if (compact) {
       CUDA_TRY(cudaStreamSynchronize(lat->stream), "autotune");
       return compact_set_shape(lat, r, pl);

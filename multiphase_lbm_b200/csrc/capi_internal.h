@@ -4,6 +4,8 @@
 #include <cuda.h>
 #include <cuda_runtime.h>
 
+#include <vector>
+
 #include "../../include/mlbm.h"
 #include "errors.h"
 #include "lattice.cuh"
@@ -39,6 +41,16 @@ struct CompactState {
   int rows = 4, planes = 8;    // requested tile height and chunk depth
   int nty = 0, nzc = 0, rows_max = 0;
   size_t smem = 0;
+  // wavefront step (wave.cuh)
+  std::vector<long long> plane_start;  // [lz + 1] first compact index of each plane
+  int4* wave_items = nullptr;          // work list
+  unsigned* wave_need = nullptr;       // [lz] density tiles per plane
+  unsigned* wave_ctl = nullptr;        // ticket[2], done[2][lz]
+  int wave_nitems = 0;
+  int wave_tile = 1024, wave_lookahead = 4;  // nodes per item, planes ahead
+  int wave_par = 0;                    // counter set of the next launch
+  int wave_grid[2] = {0, 0};           // persistent CTAs per AA phase
+  bool wave_built = false;             // work list matches tables and shape
 };
 }  // namespace mlbm
 
@@ -107,4 +119,10 @@ template <typename T>
 mlbm_status launch_compact_two_pass(mlbm_lattice* lat, const StepArgs& a,
                                     bool write_u, bool write_rho);
 bool compact_two_pass_supported(int lx, int ly, int lz, int storage);
+// Wavefront step over the compact layout (compact.cu, wave.cuh).
+template <typename T>
+mlbm_status launch_compact_wave(mlbm_lattice* lat, const StepArgs& a,
+                                bool write_u, bool write_rho);
+mlbm_status compact_set_wave_shape(mlbm_lattice* lat, int tile, int lookahead);
+void compact_reset_wave(mlbm_lattice* lat);  // after a failed wait
 }  // namespace mlbm

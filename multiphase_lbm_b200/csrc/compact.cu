@@ -10,6 +10,7 @@
 #include "capi_internal.h"
 #include "compact.cuh"
 #include "compact2.cuh"
+#include "wave.cuh"
 
 namespace mlbm {
 
@@ -115,6 +116,10 @@ mlbm_status build_tables(mlbm_lattice* lat) {
   h[nwords] = (uint32_t)run;
   if (run >= (1ull << 31))
     return set_error(MLBM_ERR_ARG, "compact step: more than 2^31 fluid nodes");
+  c.plane_start.assign(g.lz + 1, 0);
+  for (int z = 0; z <= g.lz; ++z)
+    c.plane_start[z] = h[(long long)z * g.ly * g.wpr];
+  c.wave_built = false;
   e = cudaMemcpy(c.wbase, h.data(), (nwords + 1) * sizeof(uint32_t),
                  cudaMemcpyHostToDevice);
   if (e != cudaSuccess) return cuda_fail(e, "compact tables");
@@ -308,6 +313,9 @@ void compact_free(mlbm_lattice* lat) {
   cudaFree(c.wbase);
   cudaFree(c.wtab);
   cudaFree(c.tabs);
+  cudaFree(c.wave_items);
+  cudaFree(c.wave_need);
+  cudaFree(c.wave_ctl);
   c = CompactState{};
 }
 
@@ -392,5 +400,171 @@ mlbm_status launch_compact_two_pass(mlbm_lattice* lat, const StepArgs& a,
 
 template mlbm_status launch_compact_two_pass<float>(mlbm_lattice*, const StepArgs&, bool, bool);
 template mlbm_status launch_compact_two_pass<__half>(mlbm_lattice*, const StepArgs&, bool, bool);
+
+// ---- wavefront step (wave.cuh) ------------------------------------------------
+
+namespace {
+
+// Polls of a waiting update tile before it gives up (a poll is three acquire
+// loads and a 64 ns sleep, so the wait ends within about a second).
+constexpr unsigned kWaveSpinLimit = 1u << 20;
+
+template <typename T, int PHASE, int OUT>
+const void* wave_fn() {
+  return reinterpret_cast<const void*>(&k_cwave<T, PHASE, OUT>);
+}
+
+template <typename T>
+const void* pick_wave(int phase, int out) {
+  if (phase == 0) {
+    switch (out) {
+      case OUT_NONE: return wave_fn<T, 0, OUT_NONE>();
+      case OUT_RHO: return wave_fn<T, 0, OUT_RHO>();
+      default: return wave_fn<T, 0, OUT_RHO | OUT_VEL>();
+    }
+  }
+  switch (out) {
+    case OUT_NONE: return wave_fn<T, 1, OUT_NONE>();
+    case OUT_RHO: return wave_fn<T, 1, OUT_RHO>();
+    default: return wave_fn<T, 1, OUT_RHO | OUT_VEL>();
+  }
+}
+
+// Work list of the wavefront: tiles of `tile` fluid nodes that never straddle
+// a plane, density tiles `lookahead` planes ahead of the update tiles (the
+// order is described in wave.cuh).  Every update tile's dependencies (density
+// of planes z-1, z, z+1) come earlier in the list.
+mlbm_status build_wave(mlbm_lattice* lat) {
+  CompactState& c = lat->compact;
+  const int lz = lat->g.lz;
+  const int tile = c.wave_tile, L = c.wave_lookahead;
+  std::vector<int4> items;
+  std::vector<unsigned> need(lz, 0u);
+  items.reserve((size_t)(2 * c.nfluid / tile + 2 * lz + 8));
+  std::vector<bool> emitted(lz, false);
+  auto emit = [&](int z, int kind) {
+    for (long long k0 = c.plane_start[z]; k0 < c.plane_start[z + 1]; k0 += tile) {
+      const long long k1 = std::min(k0 + tile, c.plane_start[z + 1]);
+      items.push_back(make_int4(z, kind, (int)k0, (int)k1));
+      if (kind == kWaveDensity) ++need[z];
+    }
+  };
+  auto emit_d = [&](int z) {
+    if (z < 0 || z >= lz || emitted[z]) return;
+    emitted[z] = true;
+    emit(z, kWaveDensity);
+  };
+  emit_d(lz - 1);
+  for (int z = 0; z <= L; ++z) emit_d(z);
+  for (int z = 0; z < lz; ++z) {
+    emit_d(z + 1);  // already emitted unless lookahead < 1
+    emit(z, kWaveUpdate);
+    emit_d(z + L + 1);
+  }
+  if (items.size() > (size_t)INT32_MAX)
+    return set_error(MLBM_ERR_ARG, "wavefront step: too many work items");
+  cudaError_t e = cudaStreamSynchronize(lat->stream);
+  if (e != cudaSuccess) return cuda_fail(e, "wavefront work list");
+  cudaFree(c.wave_items);
+  cudaFree(c.wave_need);
+  cudaFree(c.wave_ctl);
+  c.wave_items = nullptr;
+  c.wave_need = nullptr;
+  c.wave_ctl = nullptr;
+  e = cudaMalloc((void**)&c.wave_items, std::max<size_t>(1, items.size()) * sizeof(int4));
+  if (e == cudaSuccess) e = cudaMalloc((void**)&c.wave_need, lz * sizeof(unsigned));
+  if (e == cudaSuccess)
+    e = cudaMalloc((void**)&c.wave_ctl, (2 + 2 * (size_t)lz) * sizeof(unsigned));
+  if (e == cudaSuccess && !items.empty())
+    e = cudaMemcpy(c.wave_items, items.data(), items.size() * sizeof(int4),
+                   cudaMemcpyHostToDevice);
+  if (e == cudaSuccess)
+    e = cudaMemcpy(c.wave_need, need.data(), lz * sizeof(unsigned),
+                   cudaMemcpyHostToDevice);
+  if (e == cudaSuccess)
+    e = cudaMemset(c.wave_ctl, 0, (2 + 2 * (size_t)lz) * sizeof(unsigned));
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return cuda_fail(e, "wavefront work list");
+  }
+  c.wave_nitems = (int)items.size();
+  c.wave_par = 0;
+  // persistent grid: every CTA that fits on the device at once (per phase:
+  // the two step kernels differ in registers)
+  int sms = 0;
+  e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, lat->device);
+  for (int ph = 0; ph < 2 && e == cudaSuccess; ++ph) {
+    int per_sm = 0;
+    const void* fn = lat->storage == MLBM_STORE_F32 ? pick_wave<float>(ph, OUT_NONE)
+                                                    : pick_wave<__half>(ph, OUT_NONE);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kWaveThreads, 0);
+    c.wave_grid[ph] = std::max(1, std::min(sms * std::max(1, per_sm), c.wave_nitems));
+  }
+  if (e != cudaSuccess) return cuda_fail(e, "wavefront occupancy");
+  c.wave_built = true;
+  return MLBM_OK;
+}
+
+}  // namespace
+
+mlbm_status compact_set_wave_shape(mlbm_lattice* lat, int tile, int lookahead) {
+  CompactState& c = lat->compact;
+  c.wave_tile = tile;
+  c.wave_lookahead = lookahead;
+  c.wave_built = false;
+  return MLBM_OK;
+}
+
+void compact_reset_wave(mlbm_lattice* lat) {
+  CompactState& c = lat->compact;
+  if (c.wave_ctl)
+    cudaMemset(c.wave_ctl, 0, (2 + 2 * (size_t)lat->g.lz) * sizeof(unsigned));
+  c.wave_par = 0;
+}
+
+template <typename T>
+mlbm_status launch_compact_wave(mlbm_lattice* lat, const StepArgs& a,
+                                bool write_u, bool write_rho) {
+  CompactState& c = lat->compact;
+  if (!c.wave_built)
+    if (mlbm_status st = build_wave(lat)) return st;
+  if (c.wave_nitems == 0) return MLBM_OK;
+  const Phys& p = lat->phys;
+  const bool inj = p.rho_inject_period != 0ull &&
+                   (unsigned long long)a.step % p.rho_inject_period == 0ull;
+  const int out = write_u ? (OUT_RHO | OUT_VEL) : (write_rho ? OUT_RHO : OUT_NONE);
+  T* cpop = static_cast<T*>(c.cpop);
+  long long cs = c.cs;
+  const uint2* cinfo = c.cinfo;
+  const uint2* wtab = c.wtab;
+  float* rho = static_cast<float*>(lat->rho);
+  float* psi = static_cast<float*>(lat->psi);
+  float* vel = lat->vel;
+  Geom g = lat->g;
+  Phys pp = p;
+  StepArgs aa = a;
+  bool injv = inj;
+  WaveArgs w;
+  w.items = c.wave_items;
+  w.need = c.wave_need;
+  w.ticket = c.wave_ctl;
+  w.done = c.wave_ctl + 2;
+  w.err = lat->err;
+  w.nitems = c.wave_nitems;
+  w.lz = g.lz;
+  w.par = c.wave_par;
+  w.spin_limit = kWaveSpinLimit;
+  void* args[] = {&cpop, &cs, &cinfo, &wtab, &rho, &psi, &vel, &g, &pp, &aa, &injv, &w};
+  const cudaError_t e = cudaLaunchKernel(pick_wave<T>(lat->phase, out),
+                                         dim3(c.wave_grid[lat->phase]),
+                                         dim3(kWaveThreads),
+                                         args, 0, lat->stream);
+  if (e != cudaSuccess) return cuda_fail(e, "wavefront time-step launch");
+  c.wave_par ^= 1;
+  return MLBM_OK;
+}
+
+template mlbm_status launch_compact_wave<float>(mlbm_lattice*, const StepArgs&, bool, bool);
+template mlbm_status launch_compact_wave<__half>(mlbm_lattice*, const StepArgs&, bool, bool);
 
 }  // namespace mlbm
