@@ -107,12 +107,18 @@ mlbm_status build_tables(mlbm_lattice* lat) {
                       cudaMemcpyDeviceToHost, lat->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(lat->stream);
   if (e != cudaSuccess) return cuda_fail(e, "compact tables");
+  // every plane starts at an even compact index: a plane with an odd fluid
+  // count is followed by one unused slot (a hole), so node pairs (pair.cuh)
+  // never straddle two planes
   unsigned long long run = 0;
+  const long long words_per_plane = (long long)g.ly * g.wpr;
   for (long long i = 0; i < nwords; ++i) {
+    if (i > 0 && i % words_per_plane == 0) run += run & 1ull;
     const uint32_t v = h[i];
     h[i] = (uint32_t)run;
     run += v;
   }
+  run += run & 1ull;
   h[nwords] = (uint32_t)run;
   if (run >= (1ull << 31))
     return set_error(MLBM_ERR_ARG, "compact step: more than 2^31 fluid nodes");
@@ -129,7 +135,7 @@ mlbm_status build_tables(mlbm_lattice* lat) {
   if (e != cudaSuccess) return cuda_fail(e, "compact tables");
   k_wtab<<<(unsigned)((nwords + 256) / 256), 256, 0, lat->stream>>>(
       lat->mask, c.wbase, c.wtab, nwords);
-  c.nfluid = (long long)run;
+  c.nfluid = (long long)run;  // compact slots: fluid nodes and holes
   c.cs = std::max(64LL, (c.nfluid + 63) / 64 * 64);
   if (c.cs > c.cap) {
     cudaFree(c.cpop);
@@ -172,9 +178,12 @@ mlbm_status enter_t(mlbm_lattice* lat) {
   k_convert<T, true><<<node_grid(lat->g), node_block(), 0, lat->stream>>>(
       static_cast<T*>(lat->pop), static_cast<T*>(c.cpop), lat->nbw, c.cnb, a,
       lat->g);
+  // holes keep (0, 0): no fluid bit
+  cudaError_t e = cudaMemsetAsync(c.cinfo, 0, c.cs * sizeof(uint2), lat->stream);
+  if (e != cudaSuccess) return cuda_fail(e, "compact node table");
   k_cinfo<<<node_grid(lat->g), node_block(), 0, lat->stream>>>(lat->nbw, c.cinfo,
                                                                 a, lat->g);
-  cudaError_t e = cudaMemsetAsync(seed + c.cs, 0, 3 * c.cs * sizeof(float), lat->stream);
+  e = cudaMemsetAsync(seed + c.cs, 0, 3 * c.cs * sizeof(float), lat->stream);
   if (e != cudaSuccess) return cuda_fail(e, "compact parts");
   if (lat->phase == 0)
     k_seed_parts<T, 0><<<node_grid(lat->g), node_block(), 0, lat->stream>>>(
@@ -240,9 +249,14 @@ bool compact_supported(int lx, int ly, int lz, int storage) {
   return compact_smem_bytes(2, lx, g.wpr) <= kSmemMax;
 }
 
+// Population offsets of the compact kernels are 32-bit (pair.cuh):
+// Q * cs < 2^32 holds for every lattice of fewer than kC2MaxNodes nodes.
+// (margin: up to one hole per plane and the rounding of cs to 64)
+constexpr long long kC2MaxNodes = (1LL << 32) / Q - 4096;
+
 bool compact_two_pass_supported(int lx, int ly, int lz, int storage) {
   return storage != MLBM_STORE_F64 && lx <= kC2MaxX && ly <= kC2MaxY &&
-         lz <= kC2MaxZ;
+         lz <= kC2MaxZ && (long long)lx * ly * lz <= kC2MaxNodes;
 }
 
 mlbm_status compact_set_shape(mlbm_lattice* lat, int rows, int planes) {
@@ -362,24 +376,27 @@ namespace {
 template <typename T, int PHASE>
 void launch_c2(mlbm_lattice* lat, const StepArgs& a, bool wu, bool wr, bool inj) {
   const CompactState& c = lat->compact;
-  const CArgs ca = args_of(lat);
-  const unsigned grid = (unsigned)((c.nfluid + kC2Threads - 1) / kC2Threads);
+  const long long per_thread = c2_nodes_per_thread<PHASE>();
+  const long long threads = (c.nfluid + per_thread - 1) / per_thread;
+  const unsigned grid = (unsigned)((threads + kC2Threads - 1) / kC2Threads);
   if (grid == 0) return;
   T* cpop = static_cast<T*>(c.cpop);
+  const uint32_t cs = (uint32_t)c.cs;
+  const int nf = (int)c.nfluid;
   float* rho = static_cast<float*>(lat->rho);
   float* psi = static_cast<float*>(lat->psi);
   if (wr)
     k_cdensity<T, PHASE, true><<<grid, kC2Threads, 0, lat->stream>>>(
-        cpop, ca, c.cinfo, c.wtab, c.nfluid, rho, psi, lat->g, lat->phys, a, inj);
+        cpop, cs, c.cinfo, c.wtab, nf, rho, psi, lat->g, lat->phys, a, inj);
   else
     k_cdensity<T, PHASE, false><<<grid, kC2Threads, 0, lat->stream>>>(
-        cpop, ca, c.cinfo, c.wtab, c.nfluid, rho, psi, lat->g, lat->phys, a, inj);
+        cpop, cs, c.cinfo, c.wtab, nf, rho, psi, lat->g, lat->phys, a, inj);
   if (wu)
     k_cupdate<T, PHASE, true><<<grid, kC2Threads, 0, lat->stream>>>(
-        cpop, ca, c.cinfo, c.wtab, c.nfluid, psi, lat->vel, lat->g, lat->phys, a, inj);
+        cpop, cs, c.cinfo, c.wtab, nf, psi, lat->vel, lat->g, lat->phys, a, inj);
   else
     k_cupdate<T, PHASE, false><<<grid, kC2Threads, 0, lat->stream>>>(
-        cpop, ca, c.cinfo, c.wtab, c.nfluid, psi, lat->vel, lat->g, lat->phys, a, inj);
+        cpop, cs, c.cinfo, c.wtab, nf, psi, lat->vel, lat->g, lat->phys, a, inj);
 }
 }  // namespace
 
@@ -437,7 +454,7 @@ const void* pick_wave(int phase, int out) {
 mlbm_status build_wave(mlbm_lattice* lat) {
   CompactState& c = lat->compact;
   const int lz = lat->g.lz;
-  const int tile = c.wave_tile, L = c.wave_lookahead;
+  const int tile = (c.wave_tile + 1) & ~1, L = c.wave_lookahead;  // whole pairs
   std::vector<int4> items;
   std::vector<unsigned> need(lz, 0u);
   items.reserve((size_t)(2 * c.nfluid / tile + 2 * lz + 8));
@@ -534,7 +551,8 @@ mlbm_status launch_compact_wave(mlbm_lattice* lat, const StepArgs& a,
                    (unsigned long long)a.step % p.rho_inject_period == 0ull;
   const int out = write_u ? (OUT_RHO | OUT_VEL) : (write_rho ? OUT_RHO : OUT_NONE);
   T* cpop = static_cast<T*>(c.cpop);
-  long long cs = c.cs;
+  uint32_t cs = (uint32_t)c.cs;
+  int nf = (int)c.nfluid;
   const uint2* cinfo = c.cinfo;
   const uint2* wtab = c.wtab;
   float* rho = static_cast<float*>(lat->rho);
@@ -554,7 +572,7 @@ mlbm_status launch_compact_wave(mlbm_lattice* lat, const StepArgs& a,
   w.lz = g.lz;
   w.par = c.wave_par;
   w.spin_limit = kWaveSpinLimit;
-  void* args[] = {&cpop, &cs, &cinfo, &wtab, &rho, &psi, &vel, &g, &pp, &aa, &injv, &w};
+  void* args[] = {&cpop, &cs, &nf, &cinfo, &wtab, &rho, &psi, &vel, &g, &pp, &aa, &injv, &w};
   const cudaError_t e = cudaLaunchKernel(pick_wave<T>(lat->phase, out),
                                          dim3(c.wave_grid[lat->phase]),
                                          dim3(kWaveThreads),

@@ -5,10 +5,13 @@
 // fluid node numbered k lives at cpop[i * cs + k].  Solid nodes own no
 // storage, so DRAM moves 19 reads and 19 writes per fluid node and nothing
 // for solids.  The index of a fluid node is found from the one-bit-per-node
-// mask: wbase[r * wpr + w] is the number of fluid nodes before word w of row
-// r = z * ly + y, so k(x, y, z) = wbase[r * wpr + x / 32] +
-// popc(mask word & bits below x).  wbase has one extra entry at the end
-// (the fluid node count), so wbase[r * wpr + wpr] is the end of row r.
+// mask: wbase[r * wpr + w] is the compact index of the first fluid node at
+// or after word w of row r = z * ly + y, so k(x, y, z) = wbase[r * wpr +
+// x / 32] + popc(mask word & bits below x).  A plane with an odd fluid count
+// is followed by one unused slot (a hole), so every plane starts at an even
+// index; the end of row r is therefore wbase + popc of its last word (not
+// always the next row's start).  wbase has one extra entry at the end (the
+// slot count).
 // cnb[k] is the neighbour word of node k (kernels.cuh: bit 0 fluid, bit i
 // the pull source x - e_i fluid, bits 19-20 the drainage slab kind).
 //
@@ -173,7 +176,7 @@ __device__ __forceinline__ float stored_value(float v, float) {
 }
 template <>
 __device__ __forceinline__ float stored_value<__half>(float v, float s) {
-  return __half2float(__float2half_rn(v - s)) + s;
+  return __fadd_rn(__half2float(__float2half_rn(__fsub_rn(v, s))), s);
 }
 
 // The density injection of compute_density (include/iteration_device.cuh:
@@ -234,8 +237,14 @@ __global__ void __launch_bounds__(kCompactThreads, 2)
       const int j = e / P, w = e - j * P;
       const long long r = (long long)zq * g.ly + wrapy(y0 - 1 + j);
       uint2 v;
-      v.x = w < wpr ? __ldg(c.mask + r * wpr + w) : 0u;
-      v.y = __ldg(c.wbase + r * wpr + w);
+      if (w < wpr) {
+        v.x = __ldg(c.mask + r * wpr + w);
+        v.y = __ldg(c.wbase + r * wpr + w);
+      } else {  // (0, end of row)
+        v.x = 0u;
+        v.y = __ldg(c.wbase + r * wpr + wpr - 1) +
+              __popc(__ldg(c.mask + r * wpr + wpr - 1));
+      }
       dst[j * P + w] = v;
     }
   };

@@ -4,12 +4,14 @@
 // Same passes as kernels.cuh / update_tma.cuh (density pass: rho and psi of
 // every fluid node; update pass: force, velocity shift, BGK, AA store), with
 // the populations addressed by compact index, so DRAM moves only fluid nodes'
-// populations.  One thread per fluid node, in compact order: consecutive
-// threads hold x-consecutive fluid nodes of a row, so own-slot accesses are
-// coalesced and neighbour-slot accesses (phase 0) fall in the neighbouring
-// rows' compact ranges.  No shared memory and no barriers: every warp keeps
-// its 19 loads in flight independently.  Results are bit-identical to the
-// dense two-pass kernels (same loads, same arithmetic in the same order).
+// populations.  The local AA step runs one thread per pair of consecutive
+// fluid nodes (pair.cuh: packed FP32 arithmetic, 8-byte accesses), the
+// gather/push step one thread per node; consecutive threads hold
+// x-consecutive fluid nodes of a row, so
+// own-slot accesses are coalesced and neighbour-slot accesses (phase 0) fall
+// in the neighbouring rows' compact ranges.  No shared memory and no
+// barriers.  Results are bit-identical to the dense two-pass kernels (same
+// loads, same arithmetic in the same order).
 //
 // Per fluid node k: cinfo[k] = (neighbour word, packed coordinates
 // x | y << 11 | z << 22); psi is the dense ghost-padded array of lattice.cuh,
@@ -47,9 +49,9 @@ static __global__ void k_cinfo(const uint32_t* __restrict__ nbw,
 // (meaningful where the neighbour is fluid): the rank of x in each
 // neighbour row from wtab[word] = (mask word, wbase), then x - 1 -> rank - 1
 // and x + 1 -> rank + fluid(x), with the periodic wrap in x (row start =
-// wtab[first word].y, row end = wtab[first word + wpr].y, the next row's
-// start; wtab has one sentinel entry after the last row).  32-bit indices:
-// the table has fewer than 2^31 words.
+// wtab[first word].y; the last node of a row = wtab[last word].y +
+// popc(last word) - 1).  32-bit indices: the table has fewer than 2^31
+// words.
 __device__ __forceinline__ void neighbour_ranks(const uint2* __restrict__ wtab,
                                                 const Geom& g, int k, int x,
                                                 int y, int z, int (&nk)[Q]) {
@@ -60,11 +62,15 @@ __device__ __forceinline__ void neighbour_ranks(const uint2* __restrict__ wtab,
   const uint32_t lb = low_bits(x);
   const int wpr = g.wpr;
   const int pz = z * g.ly, pzm = zm * g.ly, pzp = zp * g.ly;
+  auto row_last = [&](int rb) {  // compact index of the row's last node
+    const uint2 e = __ldg(wtab + rb + wpr - 1);
+    return (int)e.y + __popc(e.x) - 1;
+  };
   auto rank3 = [&](int row, int& r_, int& rl, int& rh) {
     const int rb = row * wpr;
     const uint2 v = __ldg(wtab + rb + w);
     r_ = (int)v.y + __popc(v.x & lb);
-    rl = xlo ? (int)__ldg(wtab + rb + wpr).y - 1 : r_ - 1;
+    rl = xlo ? row_last(rb) : r_ - 1;
     rh = xhi ? (int)__ldg(wtab + rb).y : r_ + (int)((v.x >> xb) & 1u);
   };
   auto rank1 = [&](int row) {
@@ -73,7 +79,7 @@ __device__ __forceinline__ void neighbour_ranks(const uint2* __restrict__ wtab,
   };
   const int r0 = (pz + y) * wpr;
   nk[0] = k;
-  nk[1] = xlo ? (int)__ldg(wtab + r0 + wpr).y - 1 : k - 1;  // (-1, 0, 0)
+  nk[1] = xlo ? row_last(r0) : k - 1;                        // (-1, 0, 0)
   nk[10] = xhi ? (int)__ldg(wtab + r0).y : k + 1;           // (+1, 0, 0)
   int r_, rl, rh;
   rank3(pz + ym, r_, rl, rh);  nk[2] = r_;  nk[4] = rl; nk[14] = rh;
@@ -94,104 +100,51 @@ static __global__ void k_wtab(const uint32_t* __restrict__ mask,
   if (i <= nwords) wtab[i] = make_uint2(i < nwords ? mask[i] : 0u, wbase[i]);
 }
 
-template <typename T, int PHASE>
-__device__ __forceinline__ void cgather(const T* __restrict__ cpop, long long cs,
-                                        int k, uint32_t nb, const int (&nk)[Q],
-                                        float shift, float (&f)[Q]) {
-#pragma unroll
-  for (int i = 0; i < Q; ++i) {
-    const float s = shift * weight<float>(i);
-    int src = k, slot = i;
-    if (PHASE == 0 && i != 0 && ((nb >> i) & 1u)) {
-      src = nk[opp(i)];
-      slot = opp(i);
-    }
-    f[i] = Pop<T>::ld(cpop + slot * cs + src, s);
-  }
-}
+}  // namespace mlbm
+
+#include "pair.cuh"
+
+namespace mlbm {
+
+// The local step (AA phase 1) runs one thread per pair of fluid nodes
+// (pair.cuh, k = 2 * thread index); the gather/push step (phase 0) one thread
+// per node (k = thread index), which keeps its neighbour addresses within a
+// register budget that leaves 3 CTAs per SM.
+template <int PHASE>
+constexpr int c2_nodes_per_thread() { return PHASE == 0 ? 1 : 2; }
 
 template <typename T, int PHASE, bool WRITE_RHO>
-__global__ void __launch_bounds__(kC2Threads)
-    k_cdensity(const T* __restrict__ cpop, CArgs c,
+__global__ void __launch_bounds__(kC2Threads, 3)
+    k_cdensity(const T* __restrict__ cpop, uint32_t cs,
                const uint2* __restrict__ cinfo, const uint2* __restrict__ wtab,
-               long long nfluid,
-               float* __restrict__ rho_out, float* __restrict__ psi, Geom g,
-               Phys p, StepArgs a, bool inj) {
-  const long long kk = (long long)blockIdx.x * kC2Threads + threadIdx.x;
-  if (kk >= nfluid) return;
-  const int k = (int)kk;
-  const uint2 ci = cinfo[k];
-  const uint32_t nb = ci.x;
-  const int x = (int)(ci.y & 2047u), y = (int)((ci.y >> 11) & 2047u),
-            z = (int)(ci.y >> 22);
-  const int kind = nb_kind(nb);
-  float d;
-  if (kind) {
-    d = slab_density(p, kind);
-  } else {
-    int nk[Q];
-    if (PHASE == 0) neighbour_ranks(wtab, g, k, x, y, z, nk);
-    float f[Q];
-    cgather<T, PHASE>(cpop, c.cs, k, nb, nk, p.rho_shift, f);
-    d = 0.f;
-#pragma unroll
-    for (int i = 0; i < Q; ++i) d = radd(d, f[i]);
-    d = inject_on(p, g, a, inj, y, d);
-  }
-  if (WRITE_RHO) rho_out[node_index(g, x, y, z)] = d;
-  store_psi<float>(psi, g, x, y, z, psi_of<float>(p, d));
+               int nfluid, float* __restrict__ rho_out, float* __restrict__ psi,
+               Geom g, Phys p, StepArgs a, bool inj) {
+  const long long k = c2_nodes_per_thread<PHASE>() *
+                      ((long long)blockIdx.x * kC2Threads + threadIdx.x);
+  if (k >= nfluid) return;
+  if (PHASE == 0)
+    node_density0<T, WRITE_RHO>(cpop, cs, cinfo, wtab, (int)k, rho_out, psi, g,
+                                p, a, inj);
+  else
+    pair_density<T, 1, WRITE_RHO>(cpop, cs, cinfo, wtab, (int)k, nfluid,
+                                  rho_out, psi, g, p, a, inj);
 }
 
 template <typename T, int PHASE, bool WRITE_U>
-__global__ void __launch_bounds__(kC2Threads)
-    k_cupdate(T* __restrict__ cpop, CArgs c, const uint2* __restrict__ cinfo,
-              const uint2* __restrict__ wtab, long long nfluid,
-              const float* __restrict__ psi,
-              float* __restrict__ vel, Geom g, Phys p, StepArgs a, bool inj) {
-  const long long kk = (long long)blockIdx.x * kC2Threads + threadIdx.x;
-  if (kk >= nfluid) return;
-  const int k = (int)kk;
-  const uint2 ci = cinfo[k];
-  const uint32_t nb = ci.x;
-  const int x = (int)(ci.y & 2047u), y = (int)((ci.y >> 11) & 2047u),
-            z = (int)(ci.y >> 22);
-  const int kind = nb_kind(nb);
-  const float shift = p.rho_shift;
-  int nk[Q];
-  if (PHASE == 0) neighbour_ranks(wtab, g, k, x, y, z, nk);
-  float f[Q];
-  float ux = 0.f, uy = 0.f, uz = 0.f;
-  if (kind) {
-    slab_populations<float>(slab_density(p, kind), f);
-  } else {
-    cgather<T, PHASE>(cpop, c.cs, k, nb, nk, shift, f);
-    float d = 0.f;
-#pragma unroll
-    for (int i = 0; i < Q; ++i) d = radd(d, f[i]);
-    d = inject_on(p, g, a, inj, y, d);
-    const long long pc = psi_index(g, x, y, z);
-    const long long sy = g.pxg, sz = (long long)(g.ly + 2) * g.pxg;
-    collide<float>(
-        p, d, __ldg(psi + pc),
-        [&](int i) { return __ldg(psi + pc + ex(i) + ey(i) * sy + ez(i) * sz); },
-        f, ux, uy, uz);
-  }
-  if (WRITE_U) {
-    const long long n = node_index(g, x, y, z);
-    vel[3 * n] = ux;
-    vel[3 * n + 1] = uy;
-    vel[3 * n + 2] = uz;
-  }
-#pragma unroll
-  for (int i = 0; i < Q; ++i) {
-    const float s = shift * weight<float>(i);
-    int dst = k, slot = opp(i);
-    if (PHASE == 0 && i != 0 && ((nb >> opp(i)) & 1u)) {
-      dst = nk[i];
-      slot = i;
-    }
-    Pop<T>::st(cpop + slot * c.cs + dst, f[i], s);
-  }
+__global__ void __launch_bounds__(kC2Threads, 3)
+    k_cupdate(T* __restrict__ cpop, uint32_t cs, const uint2* __restrict__ cinfo,
+              const uint2* __restrict__ wtab, int nfluid,
+              const float* __restrict__ psi, float* __restrict__ vel, Geom g,
+              Phys p, StepArgs a, bool inj) {
+  const long long k = c2_nodes_per_thread<PHASE>() *
+                      ((long long)blockIdx.x * kC2Threads + threadIdx.x);
+  if (k >= nfluid) return;
+  if (PHASE == 0)
+    node_update0<T, WRITE_U, false>(cpop, cs, cinfo, wtab, (int)k, psi, vel, g,
+                                    p, a, inj);
+  else
+    pair_update<T, 1, WRITE_U, false>(cpop, cs, cinfo, wtab, (int)k, nfluid,
+                                      psi, vel, g, p, a, inj);
 }
 
 }  // namespace mlbm

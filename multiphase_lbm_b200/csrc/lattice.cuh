@@ -132,14 +132,17 @@ struct Pop<double> {
     *p = v;
   }
 };
+// The shift is added and subtracted with explicit rounding, so no kernel can
+// contract it with the product that forms it (every kernel, scalar or packed,
+// stores and reads back the same bits).
 template <>
 struct Pop<__half> {
   using Real = float;
   static __device__ __forceinline__ float ld(const __half* p, float shift) {
-    return __half2float(*p) + shift;
+    return __fadd_rn(__half2float(*p), shift);
   }
   static __device__ __forceinline__ void st(__half* p, float v, float shift) {
-    *p = __float2half_rn(v - shift);
+    *p = __float2half_rn(__fsub_rn(v, shift));
   }
 };
 

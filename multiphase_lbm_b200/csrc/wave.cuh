@@ -39,8 +39,10 @@
 // launch clears the set the next launch uses (its previous user has
 // finished: launches on one stream run in order).
 //
-// Results are bit-identical to the two-pass kernels: the same loads and the
-// same arithmetic in the same order per node.
+// Per node pair the work is that of the compact two-pass kernels (pair.cuh),
+// with psi read through coherent loads; results are bit-identical to the
+// two-pass kernels.  Tiles hold whole pairs: planes start at even compact
+// indices and tile sizes are even.
 #pragma once
 
 #include "compact.cuh"
@@ -54,7 +56,7 @@ constexpr int kWaveThreads = 256;
 // CTAs per SM the register allocation is sized for: the gather/scatter step
 // (AA phase 0, neighbour ranks) needs more registers than the local step.
 template <int PHASE>
-constexpr int wave_min_blocks() { return PHASE == 0 ? 3 : 4; }
+constexpr int wave_min_blocks() { return PHASE == 0 ? 2 : 3; }
 constexpr int kWaveDensity = 0, kWaveUpdate = 1;
 
 // One work item: plane z, kind (density / update), compact range [k0, k1).
@@ -72,103 +74,15 @@ struct WaveArgs {
   unsigned spin_limit;
 };
 
-// Coherent loads (no read-only path) of data written during the launch.
-__device__ __forceinline__ float ld_coherent(const float* p) {
-  float v;
-  asm volatile("ld.global.f32 %0, [%1];" : "=f"(v) : "l"(p));
-  return v;
-}
 __device__ __forceinline__ unsigned ld_acquire(const unsigned* p) {
   unsigned v;
   asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
   return v;
 }
 
-// Density of one fluid node (the body of k_cdensity).
-template <typename T, int PHASE, bool WRITE_RHO>
-__device__ __forceinline__ void wave_density(const T* cpop, long long cs,
-                                             const uint2* __restrict__ cinfo,
-                                             const uint2* __restrict__ wtab,
-                                             int k, float* rho_out, float* psi,
-                                             const Geom& g, const Phys& p,
-                                             const StepArgs& a, bool inj) {
-  const uint2 ci = __ldg(cinfo + k);
-  const uint32_t nb = ci.x;
-  const int x = (int)(ci.y & 2047u), y = (int)((ci.y >> 11) & 2047u),
-            z = (int)(ci.y >> 22);
-  const int kind = nb_kind(nb);
-  float d;
-  if (kind) {
-    d = slab_density(p, kind);
-  } else {
-    int nk[Q];
-    if (PHASE == 0) neighbour_ranks(wtab, g, k, x, y, z, nk);
-    float f[Q];
-    cgather<T, PHASE>(cpop, cs, k, nb, nk, p.rho_shift, f);
-    d = 0.f;
-#pragma unroll
-    for (int i = 0; i < Q; ++i) d = radd(d, f[i]);
-    d = inject_on(p, g, a, inj, y, d);
-  }
-  if (WRITE_RHO) rho_out[node_index(g, x, y, z)] = d;
-  store_psi<float>(psi, g, x, y, z, psi_of<float>(p, d));
-}
-
-// Force, velocity shift, BGK and AA store of one fluid node (the body of
-// k_cupdate, with psi read coherently).
-template <typename T, int PHASE, bool WRITE_U>
-__device__ __forceinline__ void wave_update(T* cpop, long long cs,
-                                            const uint2* __restrict__ cinfo,
-                                            const uint2* __restrict__ wtab,
-                                            int k, const float* psi, float* vel,
-                                            const Geom& g, const Phys& p,
-                                            const StepArgs& a, bool inj) {
-  const uint2 ci = __ldg(cinfo + k);
-  const uint32_t nb = ci.x;
-  const int x = (int)(ci.y & 2047u), y = (int)((ci.y >> 11) & 2047u),
-            z = (int)(ci.y >> 22);
-  const int kind = nb_kind(nb);
-  const float shift = p.rho_shift;
-  int nk[Q];
-  if (PHASE == 0) neighbour_ranks(wtab, g, k, x, y, z, nk);
-  float f[Q];
-  float ux = 0.f, uy = 0.f, uz = 0.f;
-  if (kind) {
-    slab_populations<float>(slab_density(p, kind), f);
-  } else {
-    cgather<T, PHASE>(cpop, cs, k, nb, nk, shift, f);
-    float d = 0.f;
-#pragma unroll
-    for (int i = 0; i < Q; ++i) d = radd(d, f[i]);
-    d = inject_on(p, g, a, inj, y, d);
-    const long long pc = psi_index(g, x, y, z);
-    const long long sy = g.pxg, sz = (long long)(g.ly + 2) * g.pxg;
-    collide<float>(
-        p, d, ld_coherent(psi + pc),
-        [&](int i) { return ld_coherent(psi + pc + ex(i) + ey(i) * sy + ez(i) * sz); },
-        f, ux, uy, uz);
-  }
-  if (WRITE_U) {
-    const long long n = node_index(g, x, y, z);
-    vel[3 * n] = ux;
-    vel[3 * n + 1] = uy;
-    vel[3 * n + 2] = uz;
-  }
-#pragma unroll
-  for (int i = 0; i < Q; ++i) {
-    const float s = shift * weight<float>(i);
-    int dst = k, slot = opp(i);
-    if (PHASE == 0 && i != 0 && ((nb >> opp(i)) & 1u)) {
-      dst = nk[i];
-      slot = i;
-    }
-    Pop<T>::st(cpop + slot * cs + dst, f[i], s);
-  }
-}
-
 template <typename T, int PHASE, int OUT>
 __global__ void __launch_bounds__(kWaveThreads, wave_min_blocks<PHASE>())
-    k_cwave(T* cpop, long long cs, const uint2* __restrict__ cinfo,
+    k_cwave(T* cpop, uint32_t cs, int nfluid, const uint2* __restrict__ cinfo,
             const uint2* __restrict__ wtab, float* rho_out, float* psi,
             float* vel, Geom g, Phys p, StepArgs a, bool inj, WaveArgs w) {
   __shared__ int s_item[2];
@@ -216,11 +130,18 @@ __global__ void __launch_bounds__(kWaveThreads, wave_min_blocks<PHASE>())
     if (t >= w.nitems) break;
     if (t < 0) continue;
     const int4 item = __ldg(w.items + t);
+    constexpr int per = PHASE == 0 ? 1 : 2;  // nodes per thread
     if (item.y == kWaveDensity) {
 #pragma unroll 1
-      for (int k = item.z + tid; k < item.w; k += kWaveThreads)
-        wave_density<T, PHASE, (OUT & OUT_RHO) != 0>(cpop, cs, cinfo, wtab, k,
-                                                      rho_out, psi, g, p, a, inj);
+      for (int k = item.z + per * tid; k < item.w; k += per * kWaveThreads) {
+        if (PHASE == 0)
+          node_density0<T, (OUT & OUT_RHO) != 0>(cpop, cs, cinfo, wtab, k,
+                                                 rho_out, psi, g, p, a, inj);
+        else
+          pair_density<T, 1, (OUT & OUT_RHO) != 0>(cpop, cs, cinfo, wtab, k,
+                                                   nfluid, rho_out, psi, g, p,
+                                                   a, inj);
+      }
       __syncthreads();
       if (tid == 0) {
         __threadfence();
@@ -228,9 +149,14 @@ __global__ void __launch_bounds__(kWaveThreads, wave_min_blocks<PHASE>())
       }
     } else {
 #pragma unroll 1
-      for (int k = item.z + tid; k < item.w; k += kWaveThreads)
-        wave_update<T, PHASE, (OUT & OUT_VEL) != 0>(cpop, cs, cinfo, wtab, k,
-                                                     psi, vel, g, p, a, inj);
+      for (int k = item.z + per * tid; k < item.w; k += per * kWaveThreads) {
+        if (PHASE == 0)
+          node_update0<T, (OUT & OUT_VEL) != 0, true>(cpop, cs, cinfo, wtab, k,
+                                                      psi, vel, g, p, a, inj);
+        else
+          pair_update<T, 1, (OUT & OUT_VEL) != 0, true>(
+              cpop, cs, cinfo, wtab, k, nfluid, psi, vel, g, p, a, inj);
+      }
     }
   }
 }
