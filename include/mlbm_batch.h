@@ -5,11 +5,15 @@
  *
  * A batch owns one mlbm_lattice per domain (same storage format, each with
  * its own size, parameters, AA phase and step origin).  mlbm_batch_iterate
- * advances every domain with one persistent density launch and one
- * persistent update launch per step over a work list of tiles of all
- * domains, replayed through a CUDA graph; results are bit-identical to the
- * same domain advanced alone with mlbm_iterate.  Domains can be added and
- * removed between iterate calls (continuous batching).
+ * advances every domain with one density launch and one update launch per
+ * step over all domains, replayed through a CUDA graph: with FP32 / FP16
+ * storage the domains live in the fluid-only (compact) layout and the
+ * launches run one thread per fluid node or node pair of every domain; with
+ * FP64 storage (or a domain beyond the compact kernels' limits) persistent
+ * launches walk a work list of tiles of the dense layout.  Results are
+ * bit-identical to the same domain advanced alone with mlbm_iterate.
+ * Domains can be added and removed between iterate calls (continuous
+ * batching).
  */
 #ifndef MLBM_BATCH_H_
 #define MLBM_BATCH_H_
@@ -50,12 +54,14 @@ mlbm_lattice* mlbm_batch_lattice(mlbm_batch* b, int32_t id);
 int64_t mlbm_batch_domain_step(const mlbm_batch* b, int32_t id);
 mlbm_status mlbm_batch_synchronize(mlbm_batch* b);
 
-/* Work-item shape: tile rows of the density and update items, planes per
- * update item, blocks per SM (0 = as many as fit), CUDA graphs on/off. */
+/* Work-item shape of the dense mode: tile rows of the density and update
+ * items, planes per update item, blocks per SM (0 = as many as fit); CUDA
+ * graphs on/off (both modes). */
 mlbm_status mlbm_batch_set_tuning(mlbm_batch* b, int32_t rows_density,
                                   int32_t rows_update, int32_t planes,
                                   int32_t blocks_per_sm, int32_t use_graphs);
-/* Time candidate shapes on the current domains and keep the fastest.  The
+/* Time candidate shapes on the current domains and keep the fastest (dense
+ * mode; the compact mode has no shape to tune and runs no trial steps).  The
  * trial steps are real steps: every domain advances by them.  out (optional,
  * 4 ints) receives rows_density, rows_update, planes, blocks_per_sm. */
 mlbm_status mlbm_batch_autotune(mlbm_batch* b, int32_t trial_steps,

@@ -6,10 +6,12 @@
 #include <chrono>
 #include <cstring>
 #include <new>
+#include <type_traits>
 #include <vector>
 
 #include "../../include/mlbm_batch.h"
 #include "batch.cuh"
+#include "batch_compact.cuh"
 #include "capi_internal.h"
 
 using namespace mlbm;
@@ -35,6 +37,14 @@ struct mlbm_batch {
   int grid_d = 0, grid_u = 0;
   // graph of kGraphSteps steps (no rho output), for the current tables
   cudaGraphExec_t graph = nullptr;
+  // compact mode (FP32 / FP16 storage, every domain within the compact
+  // kernels' limits): the domains live in the fluid-only layout and every
+  // pass is one launch over all of them (batch_compact.cuh)
+  bool compact = false;
+  CDomain* d_cdesc = nullptr;
+  long long* d_cpre = nullptr;  // [2][n + 1] block prefixes per step parity
+  int ccap = 0;
+  int grid_c = 0;
 };
 
 namespace {
@@ -74,8 +84,81 @@ const void* pick_update(int storage) {
                                      : update_fn<double>();
 }
 
+// Compact mode: every domain enters the fluid-only layout; block prefixes
+// for both step parities (one node per thread in the gather/push step, one
+// pair per thread in the local step).
+mlbm_status rebuild_compact(mlbm_batch* b) {
+  std::vector<CDomain> desc;
+  std::vector<long long> pre[2] = {std::vector<long long>(1, 0),
+                                   std::vector<long long>(1, 0)};
+  for (size_t s = 0; s < b->dom.size(); ++s) {
+    mlbm_lattice* lat = b->dom[s];
+    if (!lat) continue;
+    if (mlbm_status st = compact_enter(lat)) return st;
+    const CompactState& c = lat->compact;
+    CDomain d;
+    std::memset(&d, 0, sizeof d);
+    d.g = lat->g;
+    d.p = lat->phys;
+    d.cpop = c.cpop;
+    d.cinfo = c.cinfo;
+    d.wtab = c.wtab;
+    d.psi = static_cast<float*>(lat->psi);
+    d.rho = static_cast<float*>(lat->rho);
+    d.cs = (uint32_t)c.cs;
+    d.nfluid = (int)c.nfluid;
+    d.phase_base = b->phase_base[s];
+    d.step_origin = b->origin[s];
+    desc.push_back(d);
+    for (int par = 0; par < 2; ++par) {
+      const int ph = d.phase_base ^ par;
+      const long long threads = ph == 0 ? d.nfluid : d.nfluid / 2;
+      pre[par].push_back(pre[par].back() + (threads + kBCThreads - 1) / kBCThreads);
+    }
+  }
+  const int n = (int)desc.size();
+  if (n > kMaxBatch) return bfail(MLBM_ERR_ARG, "too many domains in a batch");
+  if (n > b->ccap) {
+    cudaFree(b->d_cdesc);
+    cudaFree(b->d_cpre);
+    b->d_cdesc = nullptr;
+    b->d_cpre = nullptr;
+    const int cap = std::max(n, 64);
+    BCUDA(cudaMalloc(&b->d_cdesc, cap * sizeof(CDomain)), "batch table");
+    BCUDA(cudaMalloc(&b->d_cpre, 2 * (cap + 1) * sizeof(long long)), "batch table");
+    b->ccap = cap;
+  }
+  std::vector<long long> both(pre[0]);
+  both.insert(both.end(), pre[1].begin(), pre[1].end());
+  if (n)
+    BCUDA(cudaMemcpyAsync(b->d_cdesc, desc.data(), n * sizeof(CDomain),
+                          cudaMemcpyHostToDevice, b->stream), "batch table");
+  BCUDA(cudaMemcpyAsync(b->d_cpre, both.data(), both.size() * sizeof(long long),
+                        cudaMemcpyHostToDevice, b->stream), "batch table");
+  BCUDA(cudaMemcpyAsync(b->d_step, &b->bstep, sizeof(long long),
+                        cudaMemcpyHostToDevice, b->stream), "batch step");
+  BCUDA(cudaStreamSynchronize(b->stream), "batch table");
+  b->nactive = n;
+  b->grid_c = (int)std::max<long long>(1, std::max(pre[0].back(), pre[1].back()));
+  b->dirty = false;
+  return MLBM_OK;
+}
+
+bool compact_mode(const mlbm_batch* b) {
+  if (b->storage == MLBM_STORE_F64) return false;
+  for (mlbm_lattice* lat : b->dom)
+    if (lat && !lat->compact.two_pass_ok) return false;
+  return true;
+}
+
 mlbm_status rebuild(mlbm_batch* b) {
   drop_graph(b);
+  b->compact = compact_mode(b);
+  if (b->compact) return rebuild_compact(b);
+  // dense mode: the domains stay on (or return to) the dense layout
+  for (mlbm_lattice* lat : b->dom)
+    if (lat)
+      if (mlbm_status st = compact_leave(lat)) return st;
   std::vector<DomainDesc> desc;
   std::vector<long long> pre_d(1, 0), pre_u(1, 0);
   for (size_t s = 0; s < b->dom.size(); ++s) {
@@ -148,6 +231,19 @@ mlbm_status rebuild(mlbm_batch* b) {
 template <typename T>
 void launch_step(mlbm_batch* b, int delta, int reverse, unsigned inject,
                  bool write_rho) {
+  if constexpr (!std::is_same<T, double>::value) {
+    if (b->compact) {
+      if (write_rho)
+        k_batch_cdensity<T, true><<<b->grid_c, kBCThreads, 0, b->stream>>>(
+            b->d_cdesc, b->d_cpre, b->nactive, b->d_step, delta, reverse, inject);
+      else
+        k_batch_cdensity<T, false><<<b->grid_c, kBCThreads, 0, b->stream>>>(
+            b->d_cdesc, b->d_cpre, b->nactive, b->d_step, delta, reverse, inject);
+      k_batch_cupdate<T><<<b->grid_c, kBCThreads, 0, b->stream>>>(
+          b->d_cdesc, b->d_cpre, b->nactive, b->d_step, delta, reverse, inject);
+      return;
+    }
+  }
   BatchArgs a;
   a.ndomains = b->nactive;
   a.By_d = b->By_d;
@@ -240,6 +336,8 @@ mlbm_status mlbm_batch_destroy(mlbm_batch* b) {
   drop_graph(b);
   for (mlbm_lattice* lat : b->dom)
     if (lat) mlbm_lattice_destroy(lat);
+  cudaFree(b->d_cdesc);
+  cudaFree(b->d_cpre);
   cudaFree(b->d_desc);
   cudaFree(b->d_pre_d);
   cudaFree(b->d_pre_u);
@@ -258,9 +356,13 @@ mlbm_status mlbm_batch_add(mlbm_batch* b, int32_t nx, int32_t ny, int32_t nz,
   mlbm_lattice* lat = nullptr;
   if (mlbm_status st = mlbm_lattice_create(nx, ny, nz, b->storage, b->device, &lat))
     return st;
-  // the batch kernels advance the dense layout: keep the domain on it
+  // a domain advanced on its own (mlbm_iterate on its lattice) uses the
+  // kernels bit-identical to the batch's: the compact two-pass step where the
+  // compact kernels fit, else the dense two-pass step
   mlbm_status st = mlbm_set_stream(lat, b->stream);
-  if (!st) st = mlbm_set_step_kernel(lat, MLBM_KERNEL_TWO_PASS);
+  if (!st)
+    st = mlbm_set_step_kernel(lat, lat->compact.two_pass_ok ? MLBM_KERNEL_COMPACT
+                                                           : MLBM_KERNEL_TWO_PASS);
   if (!st) st = mlbm_set_params(lat, params);
   if (!st) st = mlbm_upload_fluid_mask(lat, is_fluid);
   if (!st) st = mlbm_upload_rho(lat, rho);
@@ -323,7 +425,10 @@ mlbm_status mlbm_batch_iterate(mlbm_batch* b, int32_t nsteps, int32_t reverse,
   if (mlbm_status st = run_steps(b, nsteps, reverse, inject_type)) return st;
   b->bstep += nsteps;
   for (mlbm_lattice* l : b->dom)
-    if (l) l->phase = (l->phase + nsteps) & 1;
+    if (l) {
+      l->phase = (l->phase + nsteps) & 1;
+      l->compact.parts_valid = false;  // the single-pass part sums are stale
+    }
   return MLBM_OK;
 }
 
@@ -365,6 +470,18 @@ mlbm_status mlbm_batch_autotune(mlbm_batch* b, int32_t trial_steps,
                                 int32_t* out) {
   if (!b) return bfail(MLBM_ERR_ARG, "null batch");
   if (trial_steps < 1) trial_steps = 2;
+  if (b->dirty)
+    if (mlbm_status st = rebuild(b)) return st;
+  if (b->compact) {
+    // one thread per node (pair) per pass: no work-item shape to tune
+    if (out) {
+      out[0] = b->By_d;
+      out[1] = b->By_u;
+      out[2] = b->Dz;
+      out[3] = b->bps;
+    }
+    return MLBM_OK;
+  }
   struct Cand { int bd, bu, dz, bps; };
   const Cand cands[] = {{4, 4, 8, 0},  {2, 2, 8, 0},  {8, 4, 8, 0},
                         {4, 4, 1, 0},  {4, 4, 32, 0}, {4, 2, 16, 0},

@@ -17,7 +17,8 @@ def _params(capi, i, shape):
 
 
 def _alone(capi, shape, fluid, rho, params, storage, steps):
-    # the batch advances the dense layout with the two-pass kernels
+    # FP32 / FP16 batches run the compact kernels, FP64 batches the dense
+    # two-pass kernels; both are bit-identical to the dense two-pass step
     lat = capi.Lattice(shape, storage=storage)
     lat.set_step_kernel(capi.KERNEL_TWO_PASS)
     lat.set_params(params)
@@ -32,7 +33,7 @@ def _alone(capi, shape, fluid, rho, params, storage, steps):
 SHAPES = [(32, 48, 16), (48, 32, 32), (64, 16, 48), (40, 40, 40), (33, 17, 9)]
 
 
-@pytest.mark.parametrize("storage", [0, 1])
+@pytest.mark.parametrize("storage", [0, 1, 2])
 def test_batch_equals_alone(storage):
     from multiphase_lbm_b200 import batch, capi
     cases = []
