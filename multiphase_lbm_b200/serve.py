@@ -45,6 +45,9 @@ EDGES = list(range(48, 193, 16))
 SERVE_G = -5.0
 CONVERGENCE_DS = 1e-5
 CONVERGENCE_STEPS = 1000
+# Active lattice nodes beyond which arrivals wait (about twice what fills
+# every SM of a B200 with the compact kernels).
+DEFAULT_NODE_CAP = 16_000_000
 
 
 @dataclass
@@ -105,13 +108,21 @@ def _finished(req: Request) -> bool:
     return False
 
 
-def serve_batched(reqs, hbm_cap=150e9, chunk=CONVERGENCE_STEPS, log=None):
-    """Continuous batching; returns (makespan_s, requests)."""
+def serve_batched(reqs, hbm_cap=150e9, chunk=CONVERGENCE_STEPS, log=None,
+                  node_cap=DEFAULT_NODE_CAP):
+    """Continuous batching; returns (makespan_s, requests).
+
+    Arrived requests are admitted in arrival order while their lattices fit
+    under the HBM cap and the active lattices hold fewer than `node_cap`
+    nodes in total: enough resident work to keep every SM busy, but no more,
+    since requests that share the GPU beyond saturation only wait longer for
+    their results without raising throughput."""
     batches = {True: batch.Batch(capi.STORE_F16), False: batch.Batch(capi.STORE_F32)}
     pending = sorted(reqs, key=lambda r: r.arrival)
     ready = {}       # rid -> geometry built ahead of admission
     active = {}      # rid -> (req, batch, domain id, bytes)
     used = 0
+    nodes = 0        # lattice nodes of the active requests
     t0 = time.perf_counter()
     qi = 0
     while qi < len(pending) or active:
@@ -121,12 +132,14 @@ def serve_batched(reqs, hbm_cap=150e9, chunk=CONVERGENCE_STEPS, log=None):
             r = pending[qi]
             storage = capi.STORE_F16 if r.fp16_ok else capi.STORE_F32
             need = capi.lattice_bytes(r.shape, storage)
-            if used + need > hbm_cap and active:
+            vol = int(np.prod(r.shape))
+            if active and (used + need > hbm_cap or nodes + vol > node_cap):
                 break
             fl, rho, p = ready.pop(r.rid, None) or geometry(r)
             did = batches[r.fp16_ok].add(fl, rho, p)
             active[r.rid] = (r, batches[r.fp16_ok], did, need)
             used += need
+            nodes += vol
             qi += 1
         if not active:
             if qi < len(pending):
@@ -155,6 +168,7 @@ def serve_batched(reqs, hbm_cap=150e9, chunk=CONVERGENCE_STEPS, log=None):
             r, b, did, need = active.pop(rid)
             b.remove(did)
             used -= need
+            nodes -= int(np.prod(r.shape))
         if log and done:
             log(f"t={time.perf_counter() - t0:.2f}s active={len(active)} "
                 f"done+={len(done)} queue={len(pending) - qi}")
@@ -212,6 +226,8 @@ def main(argv=None) -> int:
     ap.add_argument("--rate", type=float, default=20.0)
     ap.add_argument("--budget-scale", type=float, default=0.1)
     ap.add_argument("--hbm-cap-gb", type=float, default=150.0)
+    ap.add_argument("--node-cap", type=float, default=DEFAULT_NODE_CAP,
+                    help="active lattice nodes beyond which arrivals wait")
     ap.add_argument("--seed", type=int, default=7)
     ap.add_argument("--no-fifo", action="store_true")
     ap.add_argument("--fifo-kernel", default="auto",
@@ -219,10 +235,12 @@ def main(argv=None) -> int:
     a = ap.parse_args(argv)
     log = lambda s: print(s, file=sys.stderr, flush=True)  # noqa: E731
     reqs = make_requests(a.requests, a.rate, a.seed, a.budget_scale)
-    mk, done = serve_batched(reqs, a.hbm_cap_gb * 1e9, log=log)
+    mk, done = serve_batched(reqs, a.hbm_cap_gb * 1e9, log=log,
+                             node_cap=a.node_cap)
     out = {"config": {"requests": a.requests, "rate_per_s": a.rate,
                       "budget_scale": a.budget_scale,
-                      "hbm_cap_gb": a.hbm_cap_gb, "seed": a.seed},
+                      "hbm_cap_gb": a.hbm_cap_gb, "node_cap": a.node_cap,
+                      "seed": a.seed},
            "batched": summarise(mk, done)}
     if not a.no_fifo:
         reqs2 = make_requests(a.requests, a.rate, a.seed, a.budget_scale)
