@@ -109,12 +109,14 @@ namespace mlbm {
 // The local step (AA phase 1) runs one thread per pair of fluid nodes
 // (pair.cuh, k = 2 * thread index); the gather/push step (phase 0) one thread
 // per node (k = thread index), which keeps its neighbour addresses within a
-// register budget that leaves 3 CTAs per SM.
+// register budget that leaves 3 CTAs per SM.  The density pass is held to 48
+// registers (5 CTAs per SM); on the 200^3 bench that beat 3, 4 and 6 CTAs
+// per SM for either pass.
 template <int PHASE>
 constexpr int c2_nodes_per_thread() { return PHASE == 0 ? 1 : 2; }
 
 template <typename T, int PHASE, bool WRITE_RHO>
-__global__ void __launch_bounds__(kC2Threads, 3)
+__global__ void __launch_bounds__(kC2Threads, 5)
     k_cdensity(const T* __restrict__ cpop, uint32_t cs,
                const uint2* __restrict__ cinfo, const uint2* __restrict__ wtab,
                int nfluid, float* __restrict__ rho_out, float* __restrict__ psi,
