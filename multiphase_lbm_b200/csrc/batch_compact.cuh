@@ -98,14 +98,13 @@ __global__ void __launch_bounds__(kBCThreads, 3)
   const long long t = local * kBCThreads + threadIdx.x;
   if (ph == 0) {
     if (t >= D.nfluid) return;
-    node_update0<T, false, false>(static_cast<T*>(D.cpop), D.cs, D.cinfo,
-                                  D.wtab, (int)t, D.psi, nullptr, D.g, D.p, a,
-                                  inj);
+    node_update0<T, false>(static_cast<T*>(D.cpop), D.cs, D.cinfo, D.wtab,
+                           (int)t, PsiPlain{D.psi}, nullptr, D.g, D.p, a, inj);
   } else {
     if (2 * t >= D.nfluid) return;
-    pair_update<T, 1, false, false>(static_cast<T*>(D.cpop), D.cs, D.cinfo,
-                                    D.wtab, (int)(2 * t), D.nfluid, D.psi,
-                                    nullptr, D.g, D.p, a, inj);
+    pair_update<T, 1, false>(static_cast<T*>(D.cpop), D.cs, D.cinfo, D.wtab,
+                             (int)(2 * t), D.nfluid, PsiPlain{D.psi}, nullptr,
+                             D.g, D.p, a, inj);
   }
 }
 

@@ -142,11 +142,11 @@ __global__ void __launch_bounds__(kC2Threads, 3)
                       ((long long)blockIdx.x * kC2Threads + threadIdx.x);
   if (k >= nfluid) return;
   if (PHASE == 0)
-    node_update0<T, WRITE_U, false>(cpop, cs, cinfo, wtab, (int)k, psi, vel, g,
-                                    p, a, inj);
+    node_update0<T, WRITE_U>(cpop, cs, cinfo, wtab, (int)k, PsiPlain{psi}, vel,
+                             g, p, a, inj);
   else
-    pair_update<T, 1, WRITE_U, false>(cpop, cs, cinfo, wtab, (int)k, nfluid,
-                                      psi, vel, g, p, a, inj);
+    pair_update<T, 1, WRITE_U>(cpop, cs, cinfo, wtab, (int)k, nfluid,
+                               PsiPlain{psi}, vel, g, p, a, inj);
 }
 
 }  // namespace mlbm

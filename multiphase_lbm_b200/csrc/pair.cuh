@@ -241,17 +241,29 @@ __device__ __forceinline__ void collide2(const Phys& p, float2 d, float2 psi_sel
   }
 }
 
-// psi loads: read-only path, or coherent loads where psi is written by the
-// same launch (wave.cuh).
-template <bool COHERENT>
-__device__ __forceinline__ float psi_ld(const float* p) {
-  if (COHERENT) {
+// psi readers of the update pass, given psi_index() positions:
+//   PsiPlain    the float psi array through the read-only path (psi complete
+//               before the launch);
+//   PsiCoherent the same array with ordinary coherent loads (psi written by
+//               the same launch, wave.cuh).
+// ready() is called once before the first psi read.
+struct PsiPlain {
+  const float* psi;
+  __device__ __forceinline__ void ready() const {}
+  __device__ __forceinline__ float self(uint32_t i) const { return __ldg(psi + i); }
+  __device__ __forceinline__ float nb(uint32_t i, int) const { return __ldg(psi + i); }
+};
+struct PsiCoherent {
+  const float* psi;
+  __device__ __forceinline__ void ready() const {}
+  __device__ __forceinline__ float ld(uint32_t i) const {
     float v;
-    asm volatile("ld.global.f32 %0, [%1];" : "=f"(v) : "l"(p));
+    asm volatile("ld.global.f32 %0, [%1];" : "=f"(v) : "l"(psi + i));
     return v;
   }
-  return __ldg(p);
-}
+  __device__ __forceinline__ float self(uint32_t i) const { return ld(i); }
+  __device__ __forceinline__ float nb(uint32_t i, int) const { return ld(i); }
+};
 
 // The two nodes of pair k (k even) and whether the second one exists.
 struct Pair {
@@ -329,11 +341,11 @@ __device__ __forceinline__ void pair_density(const T* cpop, uint32_t cs,
 }
 
 // Update pass of one pair (the work of k_cupdate for two nodes).
-template <typename T, int PHASE, bool WRITE_U, bool COHERENT>
+template <typename T, int PHASE, bool WRITE_U, class PsiR>
 __device__ __forceinline__ void pair_update(T* cpop, uint32_t cs,
                                             const uint2* __restrict__ cinfo,
                                             const uint2* __restrict__ wtab,
-                                            int k, int nfluid, const float* psi,
+                                            int k, int nfluid, const PsiR& pr,
                                             float* vel, const Geom& g,
                                             const Phys& p, const StepArgs& a,
                                             bool inj) {
@@ -347,12 +359,12 @@ __device__ __forceinline__ void pair_update(T* cpop, uint32_t cs,
     const uint32_t pa = (uint32_t)psi_index(g, q.a.x, q.a.y, q.a.z);
     const uint32_t pb = (uint32_t)psi_index(g, q.b.x, q.b.y, q.b.z);
     const int sy = g.pxg, sz = (g.ly + 2) * g.pxg;
+    pr.ready();
     collide2(
-        p, d, make_float2(psi_ld<COHERENT>(psi + pa), psi_ld<COHERENT>(psi + pb)),
+        p, d, make_float2(pr.self(pa), pr.self(pb)),
         [&](int i) {
           const int o = ex(i) + ey(i) * sy + ez(i) * sz;
-          return make_float2(psi_ld<COHERENT>(psi + (pa + o)),
-                             psi_ld<COHERENT>(psi + (pb + o)));
+          return make_float2(pr.nb(pa + o, i), pr.nb(pb + o, i));
         },
         f, ux, uy, uz);
   }
@@ -378,6 +390,7 @@ __device__ __forceinline__ void pair_update(T* cpop, uint32_t cs,
   }
   pair_scatter<T, PHASE>(cpop, cs, k, A, B, p.rho_shift, f);
 }
+
 
 
 // ---- one node per thread (AA phase 0) -----------------------------------------
@@ -413,11 +426,11 @@ __device__ __forceinline__ void node_density0(const T* cpop, uint32_t cs,
   store_psi<float>(psi, g, n.x, n.y, n.z, psi_of<float>(p, d));
 }
 
-template <typename T, bool WRITE_U, bool COHERENT>
+template <typename T, bool WRITE_U, class PsiR>
 __device__ __forceinline__ void node_update0(T* cpop, uint32_t cs,
                                              const uint2* __restrict__ cinfo,
                                              const uint2* __restrict__ wtab,
-                                             int k, const float* psi, float* vel,
+                                             int k, const PsiR& pr, float* vel,
                                              const Geom& g, const Phys& p,
                                              const StepArgs& a, bool inj) {
   const PairNode n = pair_node(cinfo, k);
@@ -439,11 +452,10 @@ __device__ __forceinline__ void node_update0(T* cpop, uint32_t cs,
     d = inject_on(p, g, a, inj, n.y, d);
     const uint32_t pc = (uint32_t)psi_index(g, n.x, n.y, n.z);
     const int sy = g.pxg, sz = (g.ly + 2) * g.pxg;
+    pr.ready();
     collide<float>(
-        p, d, psi_ld<COHERENT>(psi + pc),
-        [&](int i) {
-          return psi_ld<COHERENT>(psi + (pc + (ex(i) + ey(i) * sy + ez(i) * sz)));
-        },
+        p, d, pr.self(pc),
+        [&](int i) { return pr.nb(pc + (ex(i) + ey(i) * sy + ez(i) * sz), i); },
         f, ux, uy, uz);
   }
   if (WRITE_U) {

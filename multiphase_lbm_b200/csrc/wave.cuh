@@ -151,11 +151,13 @@ __global__ void __launch_bounds__(kWaveThreads, wave_min_blocks<PHASE>())
 #pragma unroll 1
       for (int k = item.z + per * tid; k < item.w; k += per * kWaveThreads) {
         if (PHASE == 0)
-          node_update0<T, (OUT & OUT_VEL) != 0, true>(cpop, cs, cinfo, wtab, k,
-                                                      psi, vel, g, p, a, inj);
+          node_update0<T, (OUT & OUT_VEL) != 0>(cpop, cs, cinfo, wtab, k,
+                                                PsiCoherent{psi}, vel, g, p, a,
+                                                inj);
         else
-          pair_update<T, 1, (OUT & OUT_VEL) != 0, true>(
-              cpop, cs, cinfo, wtab, k, nfluid, psi, vel, g, p, a, inj);
+          pair_update<T, 1, (OUT & OUT_VEL) != 0>(
+              cpop, cs, cinfo, wtab, k, nfluid, PsiCoherent{psi}, vel, g, p, a,
+              inj);
       }
     }
   }

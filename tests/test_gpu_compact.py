@@ -192,3 +192,24 @@ def test_compact_kernels_reject_what_they_cannot_run():
         lat.set_step_kernel(capi.KERNEL_SINGLE_PASS)     # needs ly >= 4
     lat.set_step_kernel(capi.KERNEL_COMPACT)
     assert capi.Lattice((16, 16, 16)).step_kernel == capi.KERNEL_COMPACT
+
+
+@pytest.mark.parametrize("storage", [0, 1])
+def test_compact_large_rows_bit_identical(storage):
+    """Rows of ~100 fluid nodes (a block of 256-512 nodes spans a few rows,
+    as in the benchmark lattice): the compact two-pass step equals the dense
+    two-pass step bit for bit, drainage slabs and velocity output included."""
+    from multiphase_lbm_b200 import capi
+    shape = (200, 96, 80)
+    fluid, rho = sphere_case(shape, seed=77, rmin=4.0, rmax=10.0,
+                             porosity=0.5, rho0=1.9, amp=0.05)
+    kw = dict(DRAIN, rho_shift=1.0)
+    outs = []
+    for kind in (capi.KERNEL_COMPACT, capi.KERNEL_TWO_PASS):
+        lat = _lattice(capi, shape, fluid, rho, kind, storage=storage, **kw)
+        lat.iterate(0, 30)
+        lat.iterate(30, 1, write_velocity=True)
+        lat.synchronize()
+        outs.append((lat.field("rho"), lat.field("f"), lat.field("velocity")))
+    for u, v in zip(*outs):
+        assert np.array_equal(u, v)
