@@ -167,11 +167,18 @@ class Lattice:
         self.h = h
 
     def close(self) -> None:
-        if getattr(self, "h", None):
-            lib().mlbm_lattice_destroy(self.h)
+        h = getattr(self, "h", None)
+        if h:
             self.h = None
+            lib().mlbm_lattice_destroy(h)
 
-    __del__ = close
+    def __del__(self):
+        # at interpreter exit the module may already be torn down; the
+        # process exit releases the device memory then
+        try:
+            self.close()
+        except Exception:  # noqa: BLE001
+            pass
 
     def __enter__(self):
         return self

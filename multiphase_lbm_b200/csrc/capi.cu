@@ -657,13 +657,10 @@ mlbm_status mlbm_phase_stats(mlbm_lattice* lat, mlbm_stats* out) {
   if (!out) return fail(MLBM_ERR_ARG, "null output");
   if (!lat->initialized) return fail(MLBM_ERR_STATE, "stats before initialize");
   if (mlbm_status st = activate(lat)) return st;
-  int nsm = 148;
-  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, lat->device);
-  const long long total = (long long)lat->g.lx * lat->g.ly * lat->g.lz;
-  int nblocks = (int)std::min<long long>((long long)nsm * 4,
-                                         (total + kStatThreads - 1) / kStatThreads);
-  if (nblocks < 1) nblocks = 1;
-  const size_t need = ((size_t)nblocks + 1) * ST_COUNT * sizeof(double);
+  const dim3 grid(lat->g.px / 32, (lat->g.ly + 7) / 8,
+                  (lat->g.lz + kStatZ - 1) / kStatZ);
+  const long long nblocks = (long long)grid.x * grid.y * grid.z;
+  const size_t need = ((size_t)nblocks + 1) * ST_COUNT * sizeof(double) + sizeof(double);
   if (lat->stats_scratch_bytes < need) {
     cudaFree(lat->stats_scratch);
     lat->stats_scratch = nullptr;
@@ -674,20 +671,22 @@ mlbm_status mlbm_phase_stats(mlbm_lattice* lat, mlbm_stats* out) {
   double* partial = lat->stats_scratch;
   double* fin = partial + (size_t)nblocks * ST_COUNT;
   if (lat->storage == MLBM_STORE_F64)
-    k_stats_partial<double><<<nblocks, kStatThreads, 0, lat->stream>>>(
-        static_cast<const double*>(lat->rho), lat->mask, lat->g, lat->phys,
+    k_stats_partial<double><<<grid, dim3(32, 8), 0, lat->stream>>>(
+        static_cast<const double*>(lat->rho), lat->nbw, lat->g, lat->phys,
         partial);
   else
-    k_stats_partial<float><<<nblocks, kStatThreads, 0, lat->stream>>>(
-        static_cast<const float*>(lat->rho), lat->mask, lat->g, lat->phys,
+    k_stats_partial<float><<<grid, dim3(32, 8), 0, lat->stream>>>(
+        static_cast<const float*>(lat->rho), lat->nbw, lat->g, lat->phys,
         partial);
-  k_stats_final<<<1, 32, 0, lat->stream>>>(partial, nblocks, fin);
+  k_stats_final<<<1, 256, 0, lat->stream>>>(partial, nblocks, lat->err, fin);
   CUDA_TRY(cudaGetLastError(), "stats launch");
-  double h[ST_COUNT];
+  double h[ST_COUNT + 1];
   CUDA_TRY(cudaMemcpyAsync(h, fin, sizeof h, cudaMemcpyDeviceToHost, lat->stream),
            "stats copy");
   CUDA_TRY(cudaStreamSynchronize(lat->stream), "stats");
-  if (mlbm_status st = check_device_error(lat)) return st;
+  // the error flag came back with the statistics
+  if (h[ST_COUNT] != 0.0)
+    if (mlbm_status st = check_device_error(lat)) return st;
   std::memset(out, 0, sizeof *out);
   out->n_fluid = (int64_t)h[ST_NF];
   out->n_liquid = (int64_t)h[ST_NL];

@@ -108,29 +108,37 @@ __global__ void k_pop_to_ref(const T* __restrict__ pop,
 enum { ST_NF, ST_NL, ST_NV, ST_NLS, ST_NLV, ST_MASS, ST_PL, ST_PV, ST_RL,
        ST_RV, ST_MINR, ST_MAXR, ST_MINP, ST_MAXP, ST_COUNT };
 
-constexpr int kStatThreads = 256;
+constexpr int kStatThreads = 256;  // blockDim (32, 8)
+constexpr int kStatZ = 16;         // planes per block
 
+__device__ __forceinline__ double stat_op(int k, double v, double o) {
+  return (k == ST_MINR || k == ST_MINP) ? fmin(v, o)
+         : (k == ST_MAXR || k == ST_MAXP) ? fmax(v, o)
+                                           : v + o;
+}
+__device__ __forceinline__ double stat_identity(int k) {
+  return (k == ST_MINR || k == ST_MINP) ? 1e9
+         : (k == ST_MAXR || k == ST_MAXP) ? -1e-9
+                                           : 0.0;
+}
+
+// One block per 32 x 8 nodes of an (x, y) plane and kStatZ planes; partial
+// sums per block, reduced in a fixed order (deterministic).  The liquid
+// boundary test reads the node's neighbour word (bit i: x - e_i is fluid) and
+// the density of every fluid neighbour, then takes the first neighbour
+// (i = 1..18) that is solid or not liquid, as calc_cluster does.
 template <typename R>
 __global__ void __launch_bounds__(kStatThreads)
-    k_stats_partial(const R* __restrict__ rho,
-                    const uint32_t* __restrict__ mask, Geom g, Phys p,
-                    double* __restrict__ partial) {
+    k_stats_partial(const R* __restrict__ rho, const uint32_t* __restrict__ nbw,
+                    Geom g, Phys p, double* __restrict__ partial) {
   double acc[ST_COUNT];
 #pragma unroll
-  for (int k = 0; k < ST_COUNT; ++k) acc[k] = 0.0;
-  acc[ST_MINR] = 1e9;
-  acc[ST_MAXR] = -1e-9;
-  acc[ST_MINP] = 1e9;
-  acc[ST_MAXP] = -1e-9;
-  const long long total = (long long)g.lx * g.ly * g.lz;
+  for (int k = 0; k < ST_COUNT; ++k) acc[k] = stat_identity(k);
+  const int x = blockIdx.x * 32 + threadIdx.x;
+  const int y = blockIdx.y * blockDim.y + threadIdx.y;
+  const int z0 = blockIdx.z * kStatZ, z1 = min(z0 + kStatZ, g.lz);
   const R rhol = R(p.rhol_spinodal), rhog = R(p.rhog_spinodal);
-  for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-       k < total; k += (long long)gridDim.x * blockDim.x) {
-    const int x = (int)(k % g.lx);
-    const long long yz = k / g.lx;
-    const int y = (int)(yz % g.ly), z = (int)(yz / g.ly);
-    if (!fluid_at(mask, g, x, y, z)) continue;
-    const R r = rho[node_index(g, x, y, z)];
+  auto node = [&](int z, uint32_t nb, R r) {
     const R pr = pressure_of<R>(p, r);
     acc[ST_NF] += 1.0;
     acc[ST_MASS] += (double)r;
@@ -138,13 +146,19 @@ __global__ void __launch_bounds__(kStatThreads)
       acc[ST_NL] += 1.0;
       acc[ST_PL] += (double)pr;
       acc[ST_RL] += (double)r;
-      // first neighbour (i = 1..18) that is solid or non-liquid decides
+      Nbr a;
+      a.init(g, x, y, z);
+      uint32_t solid = 0u, other = 0u;
+#pragma unroll
       for (int i = 1; i < Q; ++i) {
-        const int xn = wrapc(x - ex(i), g.lx), yn = wrapc(y - ey(i), g.ly),
-                  zn = wrapc(z - ez(i), g.lz);
-        if (!fluid_at(mask, g, xn, yn, zn)) { acc[ST_NLS] += 1.0; break; }
-        if (rho[node_index(g, xn, yn, zn)] < rhol) { acc[ST_NLV] += 1.0; break; }
+        if (!((nb >> i) & 1u))
+          solid |= 1u << i;
+        else if (__ldg(rho + a.idx(-ex(i), -ey(i), -ez(i))) < rhol)
+          other |= 1u << i;
       }
+      const uint32_t first = (solid | other) & (0u - (solid | other));
+      if (first & solid) acc[ST_NLS] += 1.0;
+      else if (first) acc[ST_NLV] += 1.0;
     } else if (r < rhog) {
       acc[ST_NV] += 1.0;
       acc[ST_PV] += (double)pr;
@@ -154,49 +168,82 @@ __global__ void __launch_bounds__(kStatThreads)
     acc[ST_MAXR] = fmax(acc[ST_MAXR], (double)r);
     acc[ST_MINP] = fmin(acc[ST_MINP], (double)pr);
     acc[ST_MAXP] = fmax(acc[ST_MAXP], (double)pr);
+  };
+  if (x < g.lx && y < g.ly) {
+    // four planes' node words and densities in flight at once
+    constexpr int U = 4;
+#pragma unroll 1
+    for (int zb = z0; zb < z1; zb += U) {
+      uint32_t nbv[U];
+      R rv[U];
+#pragma unroll
+      for (int j = 0; j < U; ++j) {
+        nbv[j] = 0u;
+        rv[j] = R(0);
+        if (zb + j < z1) {
+          const long long n = node_index(g, x, y, zb + j);
+          nbv[j] = __ldg(nbw + n);
+          rv[j] = __ldg(rho + n);
+        }
+      }
+#pragma unroll
+      for (int j = 0; j < U; ++j)
+        if (nbv[j] & NB_SELF) node(zb + j, nbv[j], rv[j]);
+    }
   }
   // warp then block reduction in a fixed order (deterministic)
 #pragma unroll
   for (int k = 0; k < ST_COUNT; ++k) {
     double v = acc[k];
-    for (int off = 16; off > 0; off >>= 1) {
-      const double o = __shfl_down_sync(0xffffffffu, v, off);
-      v = (k == ST_MINR || k == ST_MINP) ? fmin(v, o)
-          : (k == ST_MAXR || k == ST_MAXP) ? fmax(v, o)
-                                            : v + o;
-    }
+    for (int off = 16; off > 0; off >>= 1)
+      v = stat_op(k, v, __shfl_down_sync(0xffffffffu, v, off));
     acc[k] = v;
   }
   __shared__ double sh[kStatThreads / 32][ST_COUNT];
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int tid = threadIdx.y * 32 + threadIdx.x;
+  const int warp = tid >> 5, lane = tid & 31;
   if (lane == 0)
     for (int k = 0; k < ST_COUNT; ++k) sh[warp][k] = acc[k];
   __syncthreads();
-  if (threadIdx.x < ST_COUNT) {
-    const int k = threadIdx.x;
+  if (tid < ST_COUNT) {
+    const int k = tid;
     double v = sh[0][k];
-    for (int w = 1; w < kStatThreads / 32; ++w) {
-      const double o = sh[w][k];
-      v = (k == ST_MINR || k == ST_MINP) ? fmin(v, o)
-          : (k == ST_MAXR || k == ST_MAXP) ? fmax(v, o)
-                                            : v + o;
-    }
-    partial[(long long)blockIdx.x * ST_COUNT + k] = v;
+    for (int w = 1; w < kStatThreads / 32; ++w) v = stat_op(k, v, sh[w][k]);
+    const long long blk =
+        blockIdx.x + (long long)gridDim.x * (blockIdx.y + (long long)gridDim.y * blockIdx.z);
+    partial[blk * ST_COUNT + k] = v;
   }
 }
 
-__global__ void k_stats_final(const double* __restrict__ partial, int nblocks,
-                              double* __restrict__ out) {
-  const int k = threadIdx.x;
-  if (k >= ST_COUNT) return;
-  double v = partial[k];
-  for (int b = 1; b < nblocks; ++b) {
-    const double o = partial[(long long)b * ST_COUNT + k];
-    v = (k == ST_MINR || k == ST_MINP) ? fmin(v, o)
-        : (k == ST_MAXR || k == ST_MAXP) ? fmax(v, o)
-                                          : v + o;
+// Reduce the per-block partials (fixed-order tree: deterministic) and append
+// the lattice's device error flag, so one copy brings both back.  Each thread
+// folds whole partial records (ST_COUNT independent loads per record), then
+// the block folds the threads' results pairwise.
+__global__ void __launch_bounds__(256)
+    k_stats_final(const double* __restrict__ partial, long long nblocks,
+                  const int* __restrict__ err, double* __restrict__ out) {
+  __shared__ double sh[ST_COUNT][256];
+  const int tid = threadIdx.x;
+  double v[ST_COUNT];
+#pragma unroll
+  for (int k = 0; k < ST_COUNT; ++k) v[k] = stat_identity(k);
+  for (long long b = tid; b < nblocks; b += 256) {
+    const double* rec = partial + b * ST_COUNT;
+#pragma unroll
+    for (int k = 0; k < ST_COUNT; ++k) v[k] = stat_op(k, v[k], __ldg(rec + k));
   }
-  out[k] = v;
+#pragma unroll
+  for (int k = 0; k < ST_COUNT; ++k) sh[k][tid] = v[k];
+  __syncthreads();
+  for (int s = 128; s > 0; s >>= 1) {
+    if (tid < s)
+#pragma unroll
+      for (int k = 0; k < ST_COUNT; ++k)
+        sh[k][tid] = stat_op(k, sh[k][tid], sh[k][tid + s]);
+    __syncthreads();
+  }
+  if (tid < ST_COUNT) out[tid] = sh[tid][0];
+  if (tid == 0) out[ST_COUNT] = err ? (double)*err : 0.0;
 }
 
 // Per-x-plane fluid / liquid node counts (integer atomics: deterministic).
