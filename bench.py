@@ -284,11 +284,8 @@ def main():
     if dist:
         dist.barrier()
     ms = ev0.elapsed_time(ev1)
-    t_max = ms
-    if dist:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        t_max = float(t.item())
+    from multiphase_lbm_b200.shard import max_over_ranks
+    t_max = max_over_ranks(ms)
     s_per_step = t_max / 1e3 / args.steps
     mlups = n_nodes * world * args.steps / (t_max / 1e3) / 1e6
 
@@ -367,10 +364,8 @@ def run_e2e(capi, torch, fluid, rho, params, storage, device, steps, dist,
     check(lib().mlbm_download_field(lat.h, FIELD_RHO, DTYPE_F32,
                                     out_h.ctypes.data))
     dt = time.perf_counter() - t0
-    if dist:
-        t = torch.tensor([dt], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        dt = float(t.item())
+    from multiphase_lbm_b200.shard import max_over_ranks
+    dt = max_over_ranks(dt)
     lat.close()
     world = dist.get_world_size() if dist else 1
     n = fluid.size

@@ -22,6 +22,8 @@ Both are timed with CUDA events over `--steps` steps (a bounded sample of the
 extrapolated from the sample at the measured per-step rate.
 
 Run: python -m multiphase_lbm_b200.batchbench [--domains 512 --steps 100]
+(N GPUs: torchrun --nproc-per-node N -m multiphase_lbm_b200.batchbench; every
+rank advances its share of the domains, shard.partition.)
 """
 from __future__ import annotations
 
@@ -38,27 +40,44 @@ from . import batch, capi, host
 EDGES = list(range(32, 129, 16))
 
 
-def make_domains(n, seed=3):
+def make_domains_meta(n, seed=3):
+    """(shape, porosity, G_ads, packing seed) of every domain: cheap, so every
+    rank draws the whole list and builds only its own share."""
     rng = np.random.default_rng(seed)
     out = []
     for i in range(n):
         shape = tuple(int(v) for v in rng.choice(EDGES, 3))
         por = float(rng.uniform(0.35, 0.65))
         gads = float(rng.uniform(-2.0, 0.0))
-        fluid, _ = host.generate_packing(shape, 2.5, 7.5, por, seed * 100003 + i)
-        rhos = -math.log(1.0 - gads / -6.0)
-        params = capi.default_params(
-            G=-6.0, tau=1.0, rhos=rhos, inlet_width=max(1, round(8 * shape[0] / 200)),
-            outlet_width=1, rho_inlet=0.10, rho_outlet=1.95, rho_shift=1.0)
-        out.append((shape, fluid, np.full(shape, 2.0, np.float32), params))
+        out.append((shape, por, gads, seed * 100003 + i))
     return out
 
 
+def build_domain(shape, por, gads, pseed):
+    fluid, _ = host.generate_packing(shape, 2.5, 7.5, por, pseed)
+    rhos = -math.log(1.0 - gads / -6.0)
+    params = capi.default_params(
+        G=-6.0, tau=1.0, rhos=rhos, inlet_width=max(1, round(8 * shape[0] / 200)),
+        outlet_width=1, rho_inlet=0.10, rho_outlet=1.95, rho_shift=1.0)
+    return shape, fluid, np.full(shape, 2.0, np.float32), params
+
+
+def make_domains(n, seed=3):
+    return [build_domain(*m) for m in make_domains_meta(n, seed)]
+
+
 def run(ndomains=512, steps=100, storage=capi.STORE_F16, solve_steps=5000,
-        seed=3, log=print, compact=True) -> dict:
+        seed=3, log=print, compact=True, rank=0, world=1) -> dict:
+    """On `world` GPUs (one process each, under torchrun) every rank builds
+    and advances its own share of the domains (shard.partition by lattice
+    size); times are the slowest rank's, throughputs are whole-job."""
     import torch
+    from .shard import max_over_ranks, partition
     t0 = time.time()
-    doms = make_domains(ndomains, seed)
+    all_doms = make_domains_meta(ndomains, seed)
+    mine = partition([int(np.prod(m[0])) for m in all_doms], world)[rank]
+    doms = [build_domain(*all_doms[i]) for i in mine]
+    nodes_all = sum(int(np.prod(m[0])) for m in all_doms)
     nodes = sum(int(np.prod(s)) for s, _, _, _ in doms)
     log(f"{ndomains} domains, {nodes / 1e6:.1f} M nodes, geometry in "
         f"{time.time() - t0:.1f} s")
@@ -79,7 +98,7 @@ def run(ndomains=512, steps=100, storage=capi.STORE_F16, solve_steps=5000,
     e1.record()
     torch.cuda.synchronize()
     wall_b = time.perf_counter() - t_wall
-    ms_b = e0.elapsed_time(e1) / steps
+    ms_b = max_over_ranks(e0.elapsed_time(e1) / steps)
     mem = b.nbytes()
     b.close()
 
@@ -103,7 +122,7 @@ def run(ndomains=512, steps=100, storage=capi.STORE_F16, solve_steps=5000,
         e1.record()
         torch.cuda.synchronize()
         wall = time.perf_counter() - t_wall
-        ms = e0.elapsed_time(e1) / steps
+        ms = max_over_ranks(e0.elapsed_time(e1) / steps)
         for lat in lats:
             lat.close()
         return ms, wall
@@ -111,8 +130,10 @@ def run(ndomains=512, steps=100, storage=capi.STORE_F16, solve_steps=5000,
     ms_p, wall_p = plain(capi.KERNEL_TWO_PASS)
     ms_c, wall_c = plain(capi.KERNEL_COMPACT) if compact else (None, None)
 
+    nodes = nodes_all  # whole-job throughputs below
     res = {
         "domains": ndomains, "nodes": nodes, "storage": storage,
+        "n_gpus": world, "domains_per_rank": len(mine),
         "sample_steps": steps, "solve_steps": solve_steps,
         "batched_ms_per_step": round(ms_b, 4),
         "plain_ms_per_step": round(ms_p, 4),
@@ -137,9 +158,22 @@ def main(argv=None) -> int:
     ap.add_argument("--seed", type=int, default=3)
     a = ap.parse_args(argv)
     st = capi.STORE_F16 if a.storage == "f16" else capi.STORE_F32
-    res = run(a.domains, a.steps, st, seed=a.seed,
+    import os
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if world > 1:  # one process per GPU under torchrun
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    res = run(a.domains, a.steps, st, seed=a.seed, rank=rank, world=world,
               log=lambda s: print(s, file=sys.stderr, flush=True))
-    print(json.dumps(res))
+    if rank == 0:
+        print(json.dumps(res))
+    if world > 1:
+        dist.destroy_process_group()
     return 0
 
 
