@@ -183,7 +183,7 @@ def run_reference_arm(args, rank, world):
     ref = oracle.Reference(fluid.shape)
     ref.setup(rho, fluid, oracle.make_params(**PHYS))
     cores = len(os.sched_getaffinity(0))
-    steps_per = 2  # each bench step = a bounded sample of 2 lattice steps
+    steps_per = 1  # each bench step = a bounded sample of 1 lattice step
     for w in range(args.warmup):
         ref.step(w * steps_per, steps_per)
     t0 = time.perf_counter()
