@@ -61,6 +61,19 @@ mlbm_status mlbm_generate_packing(int32_t nx, int32_t ny, int32_t nz,
                                   float* xyzr, int64_t* count,
                                   double* porosity);
 
+/* The same packing as mlbm_generate_packing, bit for bit (same spheres,
+ * same count, same mask), with the voxelisation on GPU `device`: candidate
+ * spheres are voxelised in chunks, each node keeping the first sphere that
+ * covers it, and a prefix count of the nodes each sphere turns solid finds
+ * where the porosity target is met.  No counterpart in the reference (its
+ * packings come from a positions file or from generate_solids).  Allocates
+ * about 4 bytes per node of device memory for the call. */
+mlbm_status mlbm_generate_packing_gpu(int32_t nx, int32_t ny, int32_t nz,
+                                      float rmin, float rmax,
+                                      double porosity_target, uint64_t seed,
+                                      int64_t max_spheres, int32_t device,
+                                      uint8_t* is_fluid, float* xyzr,
+                                      int64_t* count, double* porosity);
 /* The reference's generate_solids: `num` grains from the C library rand(). */
 mlbm_status mlbm_generate_solids(uint8_t* is_fluid, int64_t* solid_number,
                                  int32_t nx, int32_t ny, int32_t nz,

@@ -25,6 +25,7 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVFLAGS = ["-O3", "-std=c++17", "-lineinfo", "--expt-relaxed-constexpr",
            "-Xcompiler", "-fPIC", "-Xcompiler", "-fopenmp",
+           "-Xcompiler", "-ffp-contract=off",
            "-I", os.path.join(ROOT, "include"), "-I", CSRC]
 
 CXX = "/usr/bin/g++"
@@ -35,7 +36,7 @@ CXXFLAGS = ["-O2", "-std=c++17", "-fPIC", "-fopenmp", "-ffp-contract=off",
             "-I", "/usr/local/cuda/include"]
 
 CUDA_SOURCES = ["capi.cu", "compat.cu", "persistent.cu", "noalloc.cu",
-                "batch.cu", "compact.cu"]
+                "batch.cu", "compact.cu", "packing.cu"]
 HOST_SOURCES = ["host/driver.cpp", "host/geometry.cpp", "host/output.cpp",
                 "host/clusters.cpp"]
 CLI_SOURCE = "host/main.cpp"

@@ -22,6 +22,10 @@ HOST_SIGNATURES = [
                                         C.c_float, C.c_float, C.c_double,
                                         C.c_uint64, C.c_int64, _VP, _VP, _VP,
                                         _VP]),
+    ("mlbm_generate_packing_gpu", C.c_int, [C.c_int32, C.c_int32, C.c_int32,
+                                            C.c_float, C.c_float, C.c_double,
+                                            C.c_uint64, C.c_int64, C.c_int32,
+                                            _VP, _VP, _VP, _VP]),
     ("mlbm_generate_solids", C.c_int, [_VP, _VP, C.c_int32, C.c_int32,
                                        C.c_int32, C.c_int32] + [C.c_float] * 8
      + [_VP]),
@@ -76,17 +80,26 @@ def init_density(shape, rho0: float, rate: float) -> np.ndarray:
 
 
 def generate_packing(shape, rmin: float, rmax: float, porosity: float,
-                     seed: int, max_spheres: int = 10_000_000):
-    """Seeded sphere packing to a porosity target: (fluid, spheres[n, 4])."""
+                     seed: int, max_spheres: int = 10_000_000, device=None):
+    """Seeded sphere packing to a porosity target: (fluid, spheres[n, 4]).
+    With `device` (a GPU index) the voxelisation runs on that GPU; the
+    result is the same, bit for bit."""
     fluid = np.ones(shape, np.uint8)
     cap = int(min(max_spheres, 2 + np.prod(shape) // 4))
     xyzr = np.zeros((cap, 4), np.float32)
     n = C.c_int64()
     por = C.c_double()
-    check(hlib().mlbm_generate_packing(*shape, rmin, rmax, porosity,
-                                       seed & (2**64 - 1), cap,
-                                       fluid.ctypes.data, xyzr.ctypes.data,
-                                       C.byref(n), C.byref(por)))
+    if device is None:
+        check(hlib().mlbm_generate_packing(*shape, rmin, rmax, porosity,
+                                           seed & (2**64 - 1), cap,
+                                           fluid.ctypes.data, xyzr.ctypes.data,
+                                           C.byref(n), C.byref(por)))
+    else:
+        check(hlib().mlbm_generate_packing_gpu(*shape, rmin, rmax, porosity,
+                                               seed & (2**64 - 1), cap,
+                                               int(device), fluid.ctypes.data,
+                                               xyzr.ctypes.data, C.byref(n),
+                                               C.byref(por)))
     return fluid, xyzr[: n.value].copy()
 
 
