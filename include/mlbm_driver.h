@@ -92,6 +92,19 @@ mlbm_status mlbm_cluster_stats(const float* rho, const uint8_t* is_fluid,
                                int64_t* liq_labels, int64_t* gas_labels,
                                mlbm_stats_row* out);
 
+/* The same statistics computed on GPU `device` (connected components by a
+ * lock-free union-find rooted at the first node of the reference's scan,
+ * cluster-solid contacts sorted on the device).  Same arguments, results and
+ * labels as mlbm_cluster_stats; the host arrays are copied in, the labels
+ * (optional) copied out.  Replaces the host-side calc_cluster
+ * (src/multiphase_lbm.cu:225-562) for large lattices (< 2^31 nodes). */
+mlbm_status mlbm_cluster_stats_gpu(const float* rho, const uint8_t* is_fluid,
+                                   const int64_t* solid_number, int32_t nx,
+                                   int32_t ny, int32_t nz, float rhol_spinodal,
+                                   float rhog_spinodal, int64_t solid_count,
+                                   int32_t device, int64_t* liq_labels,
+                                   int64_t* gas_labels, mlbm_stats_row* out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -414,9 +414,9 @@ mlbm_status mlbm_driver_params(const mlbm_driver* d, mlbm_params* p) {
 
 }  // extern "C"
 
-// Statistics of the current state: phase averages on the device, cluster
-// columns on the host (calc_cluster + write_stats, src/multiphase_lbm.cu:
-// 225-562, 1057-1083).  Averages the reference leaves untouched when a
+// Statistics of the current state: phase averages on the device, then the
+// cluster columns of the downloaded density on the device as well
+// (calc_cluster + write_stats, src/multiphase_lbm.cu:225-562, 1057-1083).  Averages the reference leaves untouched when a
 // phase is empty keep their previous values.
 mlbm_status driver_stats(mlbm_driver* d, std::vector<float>& rho_host) {
   mlbm_stats s;
@@ -440,10 +440,10 @@ mlbm_status driver_stats(mlbm_driver* d, std::vector<float>& rho_host) {
   if (mlbm_status st = mlbm_download_field(d->lat, MLBM_FIELD_RHO, MLBM_DTYPE_F32,
                                            rho_host.data()))
     return st;
-  return mlbm_cluster_stats(rho_host.data(), d->fluid.data(),
-                            d->solid_number.data(), d->lx, d->ly, d->lz,
-                            d->rhol_spinodal, d->rhog_spinodal, d->solid_count,
-                            nullptr, nullptr, &r);
+  return mlbm_cluster_stats_gpu(rho_host.data(), d->fluid.data(),
+                                d->solid_number.data(), d->lx, d->ly, d->lz,
+                                d->rhol_spinodal, d->rhog_spinodal,
+                                d->solid_count, d->device, nullptr, nullptr, &r);
 }
 
 void write_stats_row(std::ofstream& f, const mlbm_stats_row& r) {
@@ -556,3 +556,4 @@ mlbm_lattice* mlbm_driver_lattice(mlbm_driver* d) { return d ? d->lat : nullptr;
 }  // extern "C"
 
 std::string driver_result_folder(const mlbm_driver* d) { return d->result_folder; }
+int driver_device(const mlbm_driver* d) { return d->device; }

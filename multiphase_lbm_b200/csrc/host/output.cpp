@@ -12,6 +12,7 @@
 
 // The driver's result folder (driver.cpp).
 std::string driver_result_folder(const mlbm_driver* d);
+int driver_device(const mlbm_driver* d);
 
 extern "C" mlbm_status mlbm_driver_write_vtk(mlbm_driver* d, int64_t num) {
   if (!d) return mlbm::set_error(MLBM_ERR_ARG, "null driver");
@@ -37,9 +38,9 @@ extern "C" mlbm_status mlbm_driver_write_vtk(mlbm_driver* d, int64_t num) {
                    nullptr);
   std::vector<int64_t> liq(n), gas(n);
   mlbm_stats_row row{};
-  if (mlbm_status st = mlbm_cluster_stats(rho.data(), fluid, sn, lx, ly, lz,
-                                          p.rhol_spinodal, p.rhog_spinodal,
-                                          solid_count, liq.data(), gas.data(), &row))
+  if (mlbm_status st = mlbm_cluster_stats_gpu(
+          rho.data(), fluid, sn, lx, ly, lz, p.rhol_spinodal, p.rhog_spinodal,
+          solid_count, driver_device(d), liq.data(), gas.data(), &row))
     return st;
 
   char name[1024];

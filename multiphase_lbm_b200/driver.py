@@ -46,6 +46,10 @@ DRIVER_SIGNATURES = [
     ("mlbm_cluster_stats", C.c_int, [_VP, _VP, _VP, C.c_int32, C.c_int32,
                                      C.c_int32, C.c_float, C.c_float,
                                      C.c_int64, _VP, _VP, C.POINTER(StatsRow)]),
+    ("mlbm_cluster_stats_gpu", C.c_int, [_VP, _VP, _VP, C.c_int32, C.c_int32,
+                                         C.c_int32, C.c_float, C.c_float,
+                                         C.c_int64, C.c_int32, _VP, _VP,
+                                         C.POINTER(StatsRow)]),
 ]
 
 _bound = False
@@ -126,8 +130,10 @@ class Driver:
         return d
 
 
-def cluster_stats(rho, fluid, solid_number, rhol, rhog, solid_count):
-    """Cluster columns of a Stats.txt row plus liquid / gas labels."""
+def cluster_stats(rho, fluid, solid_number, rhol, rhog, solid_count,
+                  device=None):
+    """Cluster columns of a Stats.txt row plus liquid / gas labels; on the
+    host, or on GPU `device` (an int) when given."""
     shape = rho.shape
     r = np.ascontiguousarray(rho, np.float32)
     f = np.ascontiguousarray(fluid, np.uint8)
@@ -135,8 +141,13 @@ def cluster_stats(rho, fluid, solid_number, rhol, rhog, solid_count):
     liq = np.zeros(shape, np.int64)
     gas = np.zeros(shape, np.int64)
     row = StatsRow()
-    check(dlib().mlbm_cluster_stats(r.ctypes.data, f.ctypes.data, sn.ctypes.data,
-                                    *shape, rhol, rhog, solid_count,
-                                    liq.ctypes.data, gas.ctypes.data,
-                                    C.byref(row)))
+    if device is None:
+        check(dlib().mlbm_cluster_stats(
+            r.ctypes.data, f.ctypes.data, sn.ctypes.data, *shape, rhol, rhog,
+            solid_count, liq.ctypes.data, gas.ctypes.data, C.byref(row)))
+    else:
+        check(dlib().mlbm_cluster_stats_gpu(
+            r.ctypes.data, f.ctypes.data, sn.ctypes.data, *shape, rhol, rhog,
+            solid_count, int(device), liq.ctypes.data, gas.ctypes.data,
+            C.byref(row)))
     return row.as_dict(), liq, gas
