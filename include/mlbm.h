@@ -276,6 +276,50 @@ mlbm_status mlbm_phase_stats_noalloc(const float* rho_dev,
                                      const mlbm_params* params, void* stream,
                                      mlbm_stats* out);
 
+/* ---- Slab decomposition (one lattice over several GPUs) --------------------
+ * A lattice of nz planes split along z into slabs, one per GPU: a slab
+ * lattice of z-extent m + 2 holds the planes [z0 - 1, z0 + m] of the whole
+ * lattice (periodic in z), whose first and last planes are HALO planes: the
+ * step reads them but only advances the m own planes between them.  The
+ * reference has no multi-GPU path; this replaces nothing in it and keeps its
+ * step bit for bit: a decomposed run gives the undecomposed lattice's state
+ * exactly.  Compact two-pass step only (FP32 / FP16 storage).
+ *
+ * Per time step, with the AA phase p of the stored state (mlbm_lattice_info):
+ *   if p == 0: halo planes <- neighbours' edge planes   (MLBM_HALO_POP_*)
+ *   mlbm_step_pass(lat, step, 0, ...)                    density pass
+ *   psi halo planes <- neighbours' psi edge planes        (MLBM_HALO_PSI_*)
+ *   mlbm_step_pass(lat, step, 1, ...)                    update pass
+ *   if p == 0: neighbours' edge planes <- halo planes    (MLBM_HALO_POP_*)
+ * Side 0 is the lower face (local z = 0 / 1), side 1 the upper one; the
+ * EDGE segments of side 0 of one slab pair with the GHOST segments of side 1
+ * of the slab below it (and side 1 with side 0 of the slab above), segment
+ * for segment, equal sizes. */
+#define MLBM_HALO_PSI_EDGE 0  /* psi of the own plane next to the face */
+#define MLBM_HALO_PSI_GHOST 1 /* psi of the halo plane */
+#define MLBM_HALO_POP_EDGE 2  /* the 5 populations of the own edge plane that
+                                 the neighbour's nodes stream through */
+#define MLBM_HALO_POP_GHOST 3 /* the same 5 populations of the halo plane */
+#define MLBM_HALO_MAX_SEGMENTS 5
+
+/* Mark the lattice as a slab (enable = 1; its z-extent must be >= 3) or as
+ * a whole periodic lattice (0).  Call after mlbm_initialize. */
+mlbm_status mlbm_set_slab(mlbm_lattice* lat, int32_t enable);
+/* One pass of one time step in the current AA phase: pass 0 = density (rho
+ * is written), pass 1 = update (the velocity too when flags has
+ * MLBM_ITER_WRITE_VELOCITY), after which the phase flips.  step, reverse and
+ * inject_type as for mlbm_iterate.  Works on any FP32/FP16 lattice; the only
+ * way to step a slab lattice (mlbm_iterate refuses slabs). */
+mlbm_status mlbm_step_pass(mlbm_lattice* lat, int64_t step, int32_t pass,
+                           int32_t reverse, uint32_t inject_type,
+                           uint32_t flags);
+/* Device segments of one halo kind on one side: *count (<=
+ * MLBM_HALO_MAX_SEGMENTS) pointers and byte sizes, on the lattice's device.
+ * Valid until the lattice is destroyed, its mask changes or another step
+ * kernel runs.  Copy them on the lattice's stream, or synchronise it first. */
+mlbm_status mlbm_halo_segments(mlbm_lattice* lat, int32_t kind, int32_t side,
+                               void** ptrs, int64_t* bytes, int32_t* count);
+
 /* Information about the lattice: dims[3], storage, phase of the stored
  * state (0/1, see kernels), initialised flag. */
 mlbm_status mlbm_lattice_info(const mlbm_lattice* lat, int32_t* dims,

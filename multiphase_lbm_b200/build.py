@@ -36,7 +36,8 @@ CXXFLAGS = ["-O2", "-std=c++17", "-fPIC", "-fopenmp", "-ffp-contract=off",
             "-I", "/usr/local/cuda/include"]
 
 CUDA_SOURCES = ["capi.cu", "compat.cu", "persistent.cu", "noalloc.cu",
-                "batch.cu", "compact.cu", "packing.cu", "clusters_gpu.cu"]
+                "batch.cu", "compact.cu", "packing.cu", "clusters_gpu.cu",
+                "slab.cu"]
 HOST_SOURCES = ["host/driver.cpp", "host/geometry.cpp", "host/output.cpp",
                 "host/clusters.cpp"]
 CLI_SOURCE = "host/main.cpp"

@@ -20,6 +20,8 @@ FIELD_RHO, FIELD_PRESSURE, FIELD_PSI, FIELD_VELOCITY, FIELD_POPULATIONS, \
     FIELD_FLUID = range(6)
 DTYPE_F32, DTYPE_F64, DTYPE_U8 = 0, 1, 2
 ITER_WRITE_VELOCITY = 1
+HALO_PSI_EDGE, HALO_PSI_GHOST, HALO_POP_EDGE, HALO_POP_GHOST = 0, 1, 2, 3
+HALO_MAX_SEGMENTS = 5
 (KERNEL_AUTO, KERNEL_FUSED, KERNEL_TWO_PASS, KERNEL_COMPACT,
  KERNEL_SINGLE_PASS, KERNEL_WAVE) = 0, 1, 2, 3, 4, 5
 Q = 19
@@ -117,6 +119,11 @@ SIGNATURES = [
     ("mlbm_set_wave_shape", C.c_int, [_VP, C.c_int32, C.c_int32]),
     ("mlbm_get_step_kernel", C.c_int32, [_VP]),
     ("mlbm_autotune", C.c_int, [_VP, C.c_int64, C.c_int32, _VP, _VP]),
+    ("mlbm_set_slab", C.c_int, [_VP, C.c_int32]),
+    ("mlbm_step_pass", C.c_int, [_VP, C.c_int64, C.c_int32, C.c_int32,
+                                 C.c_uint32, C.c_uint32]),
+    ("mlbm_halo_segments", C.c_int, [_VP, C.c_int32, C.c_int32, _VP, _VP,
+                                     _VP]),
     ("mlbm_phase_stats_noalloc", C.c_int, [_VP, _VP, C.c_int32, C.c_int32,
                                            C.c_int32, C.POINTER(Params), _VP,
                                            C.POINTER(Stats)]),
@@ -247,6 +254,27 @@ class Lattice:
                 inject_type: int = 0, write_velocity: bool = False) -> None:
         check(lib().mlbm_iterate(self.h, step0, nsteps, reverse, inject_type,
                                  ITER_WRITE_VELOCITY if write_velocity else 0))
+
+    # ---- slab decomposition (include/mlbm.h; driven by slab.py) ----
+    def set_slab(self, enable: bool = True) -> None:
+        """Planes 0 and nz - 1 become halo planes that the step reads but
+        does not advance."""
+        check(lib().mlbm_set_slab(self.h, 1 if enable else 0))
+
+    def step_pass(self, step: int, pass_: int, reverse: int = 1,
+                  inject_type: int = 0, write_velocity: bool = False) -> None:
+        """One pass (0 density, 1 update) of time step `step`."""
+        check(lib().mlbm_step_pass(self.h, step, pass_, reverse, inject_type,
+                                   ITER_WRITE_VELOCITY if write_velocity else 0))
+
+    def halo_segments(self, kind: int, side: int):
+        """[(device pointer, bytes)] of one halo kind on one side."""
+        ptrs = (C.c_void_p * HALO_MAX_SEGMENTS)()
+        nbytes = np.zeros(HALO_MAX_SEGMENTS, np.int64)
+        n = C.c_int32()
+        check(lib().mlbm_halo_segments(self.h, kind, side, ptrs, _ptr(nbytes),
+                                       C.byref(n)))
+        return [(int(ptrs[i] or 0), int(nbytes[i])) for i in range(n.value)]
 
     def field(self, which: str, f64: bool = False) -> np.ndarray:
         code, extra = {"rho": (FIELD_RHO, ()), "pressure": (FIELD_PRESSURE, ()),

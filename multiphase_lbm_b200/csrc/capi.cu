@@ -599,6 +599,10 @@ mlbm_status mlbm_iterate(mlbm_lattice* lat, int64_t step0, int32_t nsteps,
   if (!lat->initialized)
     return fail(MLBM_ERR_STATE, "iterate before initialize");
   if (nsteps < 0) return fail(MLBM_ERR_ARG, "negative step count");
+  if (lat->slab)
+    return fail(MLBM_ERR_STATE,
+                "iterate on a slab lattice: step it with mlbm_step_pass and "
+                "exchange its halos between the passes");
   if (nsteps == 0) return MLBM_OK;
   if (mlbm_status st = activate(lat)) return st;
   switch (lat->storage) {
@@ -656,6 +660,10 @@ mlbm_status mlbm_phase_stats(mlbm_lattice* lat, mlbm_stats* out) {
   if (mlbm_status st = check_lat(lat)) return st;
   if (!out) return fail(MLBM_ERR_ARG, "null output");
   if (!lat->initialized) return fail(MLBM_ERR_STATE, "stats before initialize");
+  if (lat->slab)
+    return fail(MLBM_ERR_STATE,
+                "phase statistics of a slab would count its halo planes: "
+                "gather the slabs' own planes first");
   if (mlbm_status st = activate(lat)) return st;
   const dim3 grid(lat->g.px / 32, (lat->g.ly + 7) / 8,
                   (lat->g.lz + kStatZ - 1) / kStatZ);

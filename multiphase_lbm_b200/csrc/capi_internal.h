@@ -88,6 +88,7 @@ struct mlbm_lattice {
   mlbm::CompactState compact{};            // single-pass step (compact.cuh)
 
   int phase = 0;  // 0: post-collision at opp slots of own node; 1: pushed
+  bool slab = false;  // planes 0 and lz - 1 are halo planes (slab.cu)
   bool has_params = false, has_mask = false, has_rho = false;
   bool initialized = false;
   bool vel_valid = false;
@@ -118,6 +119,9 @@ mlbm_status launch_compact(mlbm_lattice* lat, const StepArgs& a, int out);
 template <typename T>
 mlbm_status launch_compact_two_pass(mlbm_lattice* lat, const StepArgs& a,
                                     bool write_u, bool write_rho);
+template <typename T>
+mlbm_status launch_compact_pass(mlbm_lattice* lat, const StepArgs& a, int pass,
+                                bool write_u, bool write_rho);
 bool compact_two_pass_supported(int lx, int ly, int lz, int storage);
 // Wavefront step over the compact layout (compact.cu, wave.cuh).
 template <typename T>

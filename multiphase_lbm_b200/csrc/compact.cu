@@ -373,43 +373,83 @@ template mlbm_status launch_compact<float>(mlbm_lattice*, const StepArgs&, int);
 template mlbm_status launch_compact<__half>(mlbm_lattice*, const StepArgs&, int);
 
 namespace {
-template <typename T, int PHASE>
-void launch_c2(mlbm_lattice* lat, const StepArgs& a, bool wu, bool wr, bool inj) {
+// Compact indices the step advances: all fluid nodes, or for a slab lattice
+// the planes between its two halo planes.
+void own_range(const mlbm_lattice* lat, long long& kb, long long& ke) {
   const CompactState& c = lat->compact;
-  const long long per_thread = c2_nodes_per_thread<PHASE>();
-  const long long threads = (c.nfluid + per_thread - 1) / per_thread;
-  const unsigned grid = (unsigned)((threads + kC2Threads - 1) / kC2Threads);
+  if (lat->slab) {
+    kb = c.plane_start[1];
+    ke = c.plane_start[lat->g.lz - 1];
+  } else {
+    kb = 0;
+    ke = c.nfluid;
+  }
+}
+
+unsigned c2_grid(long long kb, long long ke, long long per_thread) {
+  const long long threads = (ke - kb + per_thread - 1) / per_thread;
+  return (unsigned)((threads + kC2Threads - 1) / kC2Threads);
+}
+
+template <typename T, int PHASE>
+void launch_c2_density(mlbm_lattice* lat, const StepArgs& a, bool wr, bool inj) {
+  const CompactState& c = lat->compact;
+  long long kb, ke;
+  own_range(lat, kb, ke);
+  const unsigned grid = c2_grid(kb, ke, c2_nodes_per_thread<PHASE>());
   if (grid == 0) return;
-  T* cpop = static_cast<T*>(c.cpop);
+  const T* cpop = static_cast<const T*>(c.cpop);
   const uint32_t cs = (uint32_t)c.cs;
-  const int nf = (int)c.nfluid;
   float* rho = static_cast<float*>(lat->rho);
   float* psi = static_cast<float*>(lat->psi);
   if (wr)
     k_cdensity<T, PHASE, true><<<grid, kC2Threads, 0, lat->stream>>>(
-        cpop, cs, c.cinfo, c.wtab, nf, rho, psi, lat->g, lat->phys, a, inj);
+        cpop, cs, c.cinfo, c.wtab, (int)kb, (int)ke, rho, psi, lat->g, lat->phys,
+        a, inj);
   else
     k_cdensity<T, PHASE, false><<<grid, kC2Threads, 0, lat->stream>>>(
-        cpop, cs, c.cinfo, c.wtab, nf, rho, psi, lat->g, lat->phys, a, inj);
+        cpop, cs, c.cinfo, c.wtab, (int)kb, (int)ke, rho, psi, lat->g, lat->phys,
+        a, inj);
+}
+
+template <typename T, int PHASE>
+void launch_c2_update(mlbm_lattice* lat, const StepArgs& a, bool wu, bool inj) {
+  const CompactState& c = lat->compact;
+  long long kb, ke;
+  own_range(lat, kb, ke);
+  const unsigned grid = c2_grid(kb, ke, c2_nodes_per_thread<PHASE>());
+  if (grid == 0) return;
+  T* cpop = static_cast<T*>(c.cpop);
+  const uint32_t cs = (uint32_t)c.cs;
+  const float* psi = static_cast<const float*>(lat->psi);
   if (wu)
     k_cupdate<T, PHASE, true><<<grid, kC2Threads, 0, lat->stream>>>(
-        cpop, cs, c.cinfo, c.wtab, nf, psi, lat->vel, lat->g, lat->phys, a, inj);
+        cpop, cs, c.cinfo, c.wtab, (int)kb, (int)ke, psi, lat->vel, lat->g,
+        lat->phys, a, inj);
   else
     k_cupdate<T, PHASE, false><<<grid, kC2Threads, 0, lat->stream>>>(
-        cpop, cs, c.cinfo, c.wtab, nf, psi, lat->vel, lat->g, lat->phys, a, inj);
+        cpop, cs, c.cinfo, c.wtab, (int)kb, (int)ke, psi, lat->vel, lat->g,
+        lat->phys, a, inj);
+}
+
+bool inject_now(const mlbm_lattice* lat, const StepArgs& a) {
+  const Phys& p = lat->phys;
+  return p.rho_inject_period != 0ull &&
+         (unsigned long long)a.step % p.rho_inject_period == 0ull;
 }
 }  // namespace
 
 template <typename T>
 mlbm_status launch_compact_two_pass(mlbm_lattice* lat, const StepArgs& a,
                                     bool write_u, bool write_rho) {
-  const Phys& p = lat->phys;
-  const bool inj = p.rho_inject_period != 0ull &&
-                   (unsigned long long)a.step % p.rho_inject_period == 0ull;
-  if (lat->phase == 0)
-    launch_c2<T, 0>(lat, a, write_u, write_rho, inj);
-  else
-    launch_c2<T, 1>(lat, a, write_u, write_rho, inj);
+  const bool inj = inject_now(lat, a);
+  if (lat->phase == 0) {
+    launch_c2_density<T, 0>(lat, a, write_rho, inj);
+    launch_c2_update<T, 0>(lat, a, write_u, inj);
+  } else {
+    launch_c2_density<T, 1>(lat, a, write_rho, inj);
+    launch_c2_update<T, 1>(lat, a, write_u, inj);
+  }
   const cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(e, "compact two-pass launch");
   return MLBM_OK;
@@ -417,6 +457,27 @@ mlbm_status launch_compact_two_pass(mlbm_lattice* lat, const StepArgs& a,
 
 template mlbm_status launch_compact_two_pass<float>(mlbm_lattice*, const StepArgs&, bool, bool);
 template mlbm_status launch_compact_two_pass<__half>(mlbm_lattice*, const StepArgs&, bool, bool);
+
+// One pass of the compact two-pass step (0: density, 1: update) in the
+// lattice's current AA phase; the caller flips the phase after the update.
+template <typename T>
+mlbm_status launch_compact_pass(mlbm_lattice* lat, const StepArgs& a, int pass,
+                                bool write_u, bool write_rho) {
+  const bool inj = inject_now(lat, a);
+  if (pass == 0) {
+    if (lat->phase == 0) launch_c2_density<T, 0>(lat, a, write_rho, inj);
+    else launch_c2_density<T, 1>(lat, a, write_rho, inj);
+  } else {
+    if (lat->phase == 0) launch_c2_update<T, 0>(lat, a, write_u, inj);
+    else launch_c2_update<T, 1>(lat, a, write_u, inj);
+  }
+  const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(e, "compact pass launch");
+  return MLBM_OK;
+}
+
+template mlbm_status launch_compact_pass<float>(mlbm_lattice*, const StepArgs&, int, bool, bool);
+template mlbm_status launch_compact_pass<__half>(mlbm_lattice*, const StepArgs&, int, bool, bool);
 
 // ---- wavefront step (wave.cuh) ------------------------------------------------
 

@@ -111,7 +111,9 @@ namespace mlbm {
 // per node (k = thread index), which keeps its neighbour addresses within a
 // register budget that leaves 3 CTAs per SM.  The density pass is held to 48
 // registers (5 CTAs per SM); on the 200^3 bench that beat 3, 4 and 6 CTAs
-// per SM for either pass.
+// per SM for either pass.  Both kernels advance the compact indices
+// [kbeg, nfluid): the whole lattice, or the own planes of a slab lattice
+// (kbeg is a plane start, so it is even).
 template <int PHASE>
 constexpr int c2_nodes_per_thread() { return PHASE == 0 ? 1 : 2; }
 
@@ -119,10 +121,10 @@ template <typename T, int PHASE, bool WRITE_RHO>
 __global__ void __launch_bounds__(kC2Threads, 5)
     k_cdensity(const T* __restrict__ cpop, uint32_t cs,
                const uint2* __restrict__ cinfo, const uint2* __restrict__ wtab,
-               int nfluid, float* __restrict__ rho_out, float* __restrict__ psi,
-               Geom g, Phys p, StepArgs a, bool inj) {
-  const long long k = c2_nodes_per_thread<PHASE>() *
-                      ((long long)blockIdx.x * kC2Threads + threadIdx.x);
+               int kbeg, int nfluid, float* __restrict__ rho_out,
+               float* __restrict__ psi, Geom g, Phys p, StepArgs a, bool inj) {
+  const long long k = kbeg + c2_nodes_per_thread<PHASE>() *
+                                 ((long long)blockIdx.x * kC2Threads + threadIdx.x);
   if (k >= nfluid) return;
   if (PHASE == 0)
     node_density0<T, WRITE_RHO>(cpop, cs, cinfo, wtab, (int)k, rho_out, psi, g,
@@ -135,11 +137,11 @@ __global__ void __launch_bounds__(kC2Threads, 5)
 template <typename T, int PHASE, bool WRITE_U>
 __global__ void __launch_bounds__(kC2Threads, 3)
     k_cupdate(T* __restrict__ cpop, uint32_t cs, const uint2* __restrict__ cinfo,
-              const uint2* __restrict__ wtab, int nfluid,
+              const uint2* __restrict__ wtab, int kbeg, int nfluid,
               const float* __restrict__ psi, float* __restrict__ vel, Geom g,
               Phys p, StepArgs a, bool inj) {
-  const long long k = c2_nodes_per_thread<PHASE>() *
-                      ((long long)blockIdx.x * kC2Threads + threadIdx.x);
+  const long long k = kbeg + c2_nodes_per_thread<PHASE>() *
+                                 ((long long)blockIdx.x * kC2Threads + threadIdx.x);
   if (k >= nfluid) return;
   if (PHASE == 0)
     node_update0<T, WRITE_U>(cpop, cs, cinfo, wtab, (int)k, PsiPlain{psi}, vel,
