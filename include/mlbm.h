@@ -320,6 +320,23 @@ mlbm_status mlbm_step_pass(mlbm_lattice* lat, int64_t step, int32_t pass,
 mlbm_status mlbm_halo_segments(mlbm_lattice* lat, int32_t kind, int32_t side,
                                void** ptrs, int64_t* bytes, int32_t* count);
 
+/* The halo moves among slabs held by one process as ONE kernel per
+ * exchange: `ring` lists the slabs in z order (periodic); every slab's memory
+ * must be reachable from the device of slabs[0], which runs the kernel (the
+ * same device, or devices with peer access, which create enables).  The
+ * exchange waits for every slab's stream and every slab's stream waits for
+ * it.  what: MLBM_RING_POP_IN (before an AA phase-0 step), MLBM_RING_PSI
+ * (between the passes), MLBM_RING_POP_OUT (after a phase-0 update; merges
+ * each received slot only where its pusher is fluid). */
+typedef struct mlbm_slab_ring mlbm_slab_ring;
+#define MLBM_RING_POP_IN 0
+#define MLBM_RING_PSI 1
+#define MLBM_RING_POP_OUT 2
+mlbm_status mlbm_slab_ring_create(mlbm_lattice* const* slabs, int32_t n,
+                                  mlbm_slab_ring** out);
+mlbm_status mlbm_slab_ring_exchange(mlbm_slab_ring* ring, int32_t what);
+mlbm_status mlbm_slab_ring_destroy(mlbm_slab_ring* ring);
+
 /* Information about the lattice: dims[3], storage, phase of the stored
  * state (0/1, see kernels), initialised flag. */
 mlbm_status mlbm_lattice_info(const mlbm_lattice* lat, int32_t* dims,

@@ -124,6 +124,9 @@ SIGNATURES = [
                                  C.c_uint32, C.c_uint32]),
     ("mlbm_halo_segments", C.c_int, [_VP, C.c_int32, C.c_int32, _VP, _VP,
                                      _VP]),
+    ("mlbm_slab_ring_create", C.c_int, [_VP, C.c_int32, C.POINTER(_VP)]),
+    ("mlbm_slab_ring_exchange", C.c_int, [_VP, C.c_int32]),
+    ("mlbm_slab_ring_destroy", C.c_int, [_VP]),
     ("mlbm_phase_stats_noalloc", C.c_int, [_VP, _VP, C.c_int32, C.c_int32,
                                            C.c_int32, C.POINTER(Params), _VP,
                                            C.POINTER(Stats)]),

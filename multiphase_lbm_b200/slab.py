@@ -23,6 +23,8 @@ contiguous range (a padded psi plane; one population slot of one plane of
 the fluid-only layout) and moves with one copy or one send, no packing.
 
 Transports:
+* :class:`RingExchange` -- all slabs in this process, one kernel per
+  exchange (``mlbm_slab_ring``, peer loads and stores between GPUs);
 * :class:`LocalExchange` -- all slabs in this process: device-to-device
   copies on the current torch stream (the slabs' lattices run on it too);
 * :class:`RankExchange` -- one slab per rank (torchrun): the same moves as
@@ -213,6 +215,46 @@ class LocalExchange:
         self._move(GHOST_POP, EDGE_POP, MOVES_OUT)
 
 
+class RingExchange:
+    """All slabs of this process, one kernel per exchange
+    (``mlbm_slab_ring``): the same moves and merge as
+    :class:`LocalExchange`, issued from C as one launch, with the slabs on
+    one GPU or on GPUs with peer access (loads and stores over NVLink)."""
+
+    def __init__(self, slabs: Sequence[Slab]):
+        import ctypes as C
+        self.slabs = list(slabs)
+        arr = (C.c_void_p * len(self.slabs))(*[s.lat.h.value for s in self.slabs])
+        h = C.c_void_p()
+        capi.check(capi.lib().mlbm_slab_ring_create(arr, len(self.slabs),
+                                                    C.byref(h)))
+        self.h = h
+
+    def _run(self, what: int) -> None:
+        capi.check(capi.lib().mlbm_slab_ring_exchange(self.h, what))
+
+    def pops_in(self) -> None:
+        self._run(0)
+
+    def psi(self) -> None:
+        self._run(1)
+
+    def pops_out(self) -> None:
+        self._run(2)
+
+    def close(self) -> None:
+        h = getattr(self, "h", None)
+        if h:
+            self.h = None
+            capi.lib().mlbm_slab_ring_destroy(h)
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:  # noqa: BLE001
+            pass
+
+
 class RankExchange:
     """Halo moves between ranks of a process group, one slab per rank, rank
     order = z order (periodic).  Each exchange is one batch of sends and
@@ -306,14 +348,20 @@ class SlabRun:
 
 def decompose(fluid: np.ndarray, rho: np.ndarray, params, parts: int,
               storage: int = capi.STORE_F32,
-              devices: Optional[Sequence[int]] = None) -> SlabRun:
+              devices: Optional[Sequence[int]] = None,
+              transport: str = "ring") -> SlabRun:
     """All slabs of a lattice in this process (`devices[i]` for slab i,
-    default GPU 0), exchanging through :class:`LocalExchange`."""
+    default GPU 0), exchanging through :class:`RingExchange` ("ring", one
+    kernel per exchange) or :class:`LocalExchange` ("local", torch ops)."""
     bounds = slab_bounds(fluid, parts)
     devs = list(devices) if devices is not None else [0] * parts
     slabs = [Slab(fluid, rho, params, z0, m, storage, devs[i])
              for i, (z0, m) in enumerate(bounds)]
-    return SlabRun(slabs, LocalExchange(slabs))
+    if transport == "ring":
+        return SlabRun(slabs, RingExchange(slabs))
+    if transport == "local":
+        return SlabRun(slabs, LocalExchange(slabs))
+    raise ValueError(f"unknown transport {transport!r}")
 
 
 def gather(slabs: Sequence[Slab], which: str) -> np.ndarray:

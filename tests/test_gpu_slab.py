@@ -4,7 +4,8 @@ their halos between the passes must reproduce the undecomposed lattice bit
 for bit -- populations, density and velocity -- through both AA phases, for
 FP32 and FP16 storage, even and uneven splits, one-plane slabs, drainage
 slabs and injection.  The slabs run one after another on one stream with
-device copies as the transport (no kernel waits on another)."""
+the transport: the ring kernel (one launch per exchange) or torch copies; no
+kernel waits on another."""
 import numpy as np
 import pytest
 
@@ -25,7 +26,7 @@ def _whole(capi, fluid, rho, storage, params):
     return lat
 
 
-def _compare(shape, parts, storage, steps, params_kw, seed=5):
+def _compare(shape, parts, storage, steps, params_kw, seed=5, transport="ring"):
     import torch
 
     from multiphase_lbm_b200 import capi, slab
@@ -33,7 +34,8 @@ def _compare(shape, parts, storage, steps, params_kw, seed=5):
                              porosity=0.55, rho0=1.9, amp=0.05)
     params = capi.default_params(**params_kw)
     whole = _whole(capi, fluid, rho, storage, params)
-    run = slab.decompose(fluid, rho, params, parts, storage)
+    run = slab.decompose(fluid, rho, params, parts, storage,
+                         transport=transport)
     try:
         whole.iterate(0, steps, write_velocity=True)
         run.run(0, steps - 1)
@@ -50,17 +52,20 @@ def _compare(shape, parts, storage, steps, params_kw, seed=5):
         whole.close()
 
 
+@pytest.mark.parametrize("transport", ["ring", "local"])
 @pytest.mark.parametrize("parts", [2, 3, 4])
 @pytest.mark.parametrize("steps", [1, 2, 7])
-def test_slabs_match_whole_lattice_fp32(parts, steps):
+def test_slabs_match_whole_lattice_fp32(parts, steps, transport):
     from multiphase_lbm_b200 import capi
-    _compare((40, 36, 32), parts, capi.STORE_F32, steps, DRAIN)
+    _compare((40, 36, 32), parts, capi.STORE_F32, steps, DRAIN,
+             transport=transport)
 
 
+@pytest.mark.parametrize("transport", ["ring", "local"])
 @pytest.mark.parametrize("parts", [2, 3])
-def test_slabs_match_whole_lattice_fp16(parts):
+def test_slabs_match_whole_lattice_fp16(parts, transport):
     from multiphase_lbm_b200 import capi
-    _compare((40, 36, 32), parts, capi.STORE_F16, 8, DRAIN)
+    _compare((40, 36, 32), parts, capi.STORE_F16, 8, DRAIN, transport=transport)
 
 
 def test_one_plane_slabs_and_odd_rows():
