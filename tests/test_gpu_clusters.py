@@ -138,3 +138,27 @@ def test_drainage_sized_lattice_matches_host():
     rho = (0.15 + 6.0 * _smooth(shape, 11, 4)).astype(np.float32)
     got = _check(rho, fl, sn, ns)
     assert got["liq_cluster_count"] > 1 and got["gas_cluster_count"] > 1
+
+
+def test_simulated_drainage_field_matches_host():
+    """Clusters of a density field the lattice itself produced (64^3
+    packing, 300 drainage steps), not only synthetic fields."""
+    from conftest import sphere_case
+
+    from multiphase_lbm_b200 import capi
+    shape = (64, 64, 64)
+    fluid, rho0 = sphere_case(shape, seed=21, rmin=3.0, rmax=7.0,
+                              porosity=0.55, rho0=1.9, amp=0.05)
+    lat = capi.Lattice(shape)
+    lat.set_params(capi.default_params(G=-5.0, rhos=0.223144, tau=1.0,
+                                       inlet_width=4, outlet_width=1,
+                                       rho_inlet=0.10, rho_outlet=1.95))
+    lat.upload(fluid, rho0)
+    lat.initialize()
+    lat.iterate(0, 300)
+    rho = lat.field("rho")
+    lat.close()
+    sn = np.where(fluid == 0, 1 + (np.arange(fluid.size).reshape(shape) % 9),
+                  0).astype(np.int64)
+    got = _check(rho, fluid, sn, 9)
+    assert got["liq_cluster_count"] >= 1
