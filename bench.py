@@ -344,10 +344,16 @@ def main():
 
 def run_e2e(capi, torch, fluid, rho, params, storage, device, steps, dist,
             kernel_id=0):
-    """MLUPS through the public C ABI with host buffers (pinned)."""
+    """MLUPS through the public C ABI with host buffers (pinned).  Every
+    step's phase statistics are read back: enqueued without waiting
+    (mlbm_phase_stats_async) and read on the host one step later, while the
+    next step runs, so the GPU does not idle on the host's read."""
     fl_h = torch.from_numpy(fluid).pin_memory().numpy()
     rho_h = torch.from_numpy(rho).pin_memory().numpy()
     out_h = torch.empty(fluid.shape, dtype=torch.float32).pin_memory().numpy()
+    raw = [torch.zeros(capi.STATS_RAW_LEN, dtype=torch.float64).pin_memory().numpy()
+           for _ in range(2)]
+    done = [torch.cuda.Event() for _ in range(2)]
     lat = capi.Lattice(fluid.shape, storage=storage, device=device)
     lat.set_step_kernel(kernel_id)
     lat.set_params(params)
@@ -357,9 +363,16 @@ def run_e2e(capi, torch, fluid, rho, params, storage, device, steps, dist,
     t0 = time.perf_counter()
     lat.upload(fl_h, rho_h)
     lat.initialize()
+    sat = []
     for k in range(steps):
         lat.iterate(k, 1)
-        lat.stats()  # device->host read of the step's phase statistics
+        lat.stats_async(raw[k % 2])  # device->host read of the step's stats
+        done[k % 2].record()
+        if k > 0:
+            done[(k - 1) % 2].synchronize()
+            sat.append(lat.stats_from_raw(raw[(k - 1) % 2])["saturation"])
+    done[(steps - 1) % 2].synchronize()
+    sat.append(lat.stats_from_raw(raw[(steps - 1) % 2])["saturation"])
     from multiphase_lbm_b200.capi import DTYPE_F32, FIELD_RHO, check, lib
     check(lib().mlbm_download_field(lat.h, FIELD_RHO, DTYPE_F32,
                                     out_h.ctypes.data))
@@ -369,8 +382,8 @@ def run_e2e(capi, torch, fluid, rho, params, storage, device, steps, dist,
     lat.close()
     world = dist.get_world_size() if dist else 1
     n = fluid.size
-    import ctypes
-    stats_bytes = ctypes.sizeof(capi.Stats)
+    stats_bytes = 8 * capi.STATS_RAW_LEN
+    assert len(sat) == steps
     return {"value": round(n * world * steps / dt / 1e6, 2), "unit": "MLUPS",
             "h2d_bytes_per_step": int((n + 4 * n) / steps),
             "d2h_bytes_per_step": int(stats_bytes + 4 * n / steps)}

@@ -250,6 +250,19 @@ mlbm_status mlbm_download_field_device(mlbm_lattice* lat, int32_t field,
 /* Phase statistics of the current state (device reduction, deterministic).
  * Synchronous. */
 mlbm_status mlbm_phase_stats(mlbm_lattice* lat, mlbm_stats* out);
+/* The same statistics without waiting, for a host loop that reads every
+ * step's statistics while the next step already runs: enqueues the reduction
+ * on the lattice's stream and an asynchronous copy of MLBM_STATS_RAW_LEN
+ * doubles into `raw` (host memory; page-locked, or the copy waits).  Once
+ * the stream has passed the call (an event recorded after it, or
+ * mlbm_synchronize), mlbm_stats_from_raw gives the mlbm_stats that
+ * mlbm_phase_stats would have returned at that point of the stream, and
+ * reports a device error the step kernels flagged.  Calls in flight share
+ * one device scratch area in stream order, so any number may be queued. */
+#define MLBM_STATS_RAW_LEN 15
+mlbm_status mlbm_phase_stats_async(mlbm_lattice* lat, double* raw);
+mlbm_status mlbm_stats_from_raw(mlbm_lattice* lat, const double* raw,
+                                mlbm_stats* out);
 /* Per-x-plane counts of fluid and liquid nodes (int64[nx] each).  Sync. */
 mlbm_status mlbm_plane_profile(mlbm_lattice* lat, int64_t* n_fluid_x,
                                int64_t* n_liquid_x);

@@ -22,6 +22,7 @@ DTYPE_F32, DTYPE_F64, DTYPE_U8 = 0, 1, 2
 ITER_WRITE_VELOCITY = 1
 HALO_PSI_EDGE, HALO_PSI_GHOST, HALO_POP_EDGE, HALO_POP_GHOST = 0, 1, 2, 3
 HALO_MAX_SEGMENTS = 5
+STATS_RAW_LEN = 15
 (KERNEL_AUTO, KERNEL_FUSED, KERNEL_TWO_PASS, KERNEL_COMPACT,
  KERNEL_SINGLE_PASS, KERNEL_WAVE) = 0, 1, 2, 3, 4, 5
 Q = 19
@@ -124,6 +125,8 @@ SIGNATURES = [
                                  C.c_uint32, C.c_uint32]),
     ("mlbm_halo_segments", C.c_int, [_VP, C.c_int32, C.c_int32, _VP, _VP,
                                      _VP]),
+    ("mlbm_phase_stats_async", C.c_int, [_VP, _VP]),
+    ("mlbm_stats_from_raw", C.c_int, [_VP, _VP, C.POINTER(Stats)]),
     ("mlbm_slab_ring_create", C.c_int, [_VP, C.c_int32, C.POINTER(_VP)]),
     ("mlbm_slab_ring_exchange", C.c_int, [_VP, C.c_int32]),
     ("mlbm_slab_ring_destroy", C.c_int, [_VP]),
@@ -297,6 +300,20 @@ class Lattice:
     def stats(self) -> dict:
         s = Stats()
         check(lib().mlbm_phase_stats(self.h, C.byref(s)))
+        return s.as_dict()
+
+    def stats_async(self, raw: np.ndarray) -> None:
+        """Enqueue the phase statistics into `raw` (float64[STATS_RAW_LEN],
+        page-locked host memory) without waiting; read them with
+        :meth:`stats_from_raw` once the lattice's stream has passed this
+        call."""
+        if raw.dtype != np.float64 or raw.size < STATS_RAW_LEN:
+            raise ValueError(f"raw must be float64[{STATS_RAW_LEN}]")
+        check(lib().mlbm_phase_stats_async(self.h, _ptr(raw)))
+
+    def stats_from_raw(self, raw: np.ndarray) -> dict:
+        s = Stats()
+        check(lib().mlbm_stats_from_raw(self.h, _ptr(raw), C.byref(s)))
         return s.as_dict()
 
     def plane_profile(self):

@@ -656,9 +656,15 @@ mlbm_status mlbm_download_field(mlbm_lattice* lat, int32_t field,
   return check_device_error(lat);
 }
 
-mlbm_status mlbm_phase_stats(mlbm_lattice* lat, mlbm_stats* out) {
+}  // extern "C"
+
+namespace {
+
+// Enqueue the phase statistics reduction and the copy of its ST_COUNT + 1
+// doubles (the last one the device error flag) to host memory `h`.
+mlbm_status stats_enqueue(mlbm_lattice* lat, double* h) {
   if (mlbm_status st = check_lat(lat)) return st;
-  if (!out) return fail(MLBM_ERR_ARG, "null output");
+  if (!h) return fail(MLBM_ERR_ARG, "null output");
   if (!lat->initialized) return fail(MLBM_ERR_STATE, "stats before initialize");
   if (lat->slab)
     return fail(MLBM_ERR_STATE,
@@ -670,6 +676,8 @@ mlbm_status mlbm_phase_stats(mlbm_lattice* lat, mlbm_stats* out) {
   const long long nblocks = (long long)grid.x * grid.y * grid.z;
   const size_t need = ((size_t)nblocks + 1) * ST_COUNT * sizeof(double) + sizeof(double);
   if (lat->stats_scratch_bytes < need) {
+    // a larger area: earlier calls may still be reading the old one
+    CUDA_TRY(cudaStreamSynchronize(lat->stream), "stats");
     cudaFree(lat->stats_scratch);
     lat->stats_scratch = nullptr;
     lat->stats_scratch_bytes = 0;
@@ -688,10 +696,13 @@ mlbm_status mlbm_phase_stats(mlbm_lattice* lat, mlbm_stats* out) {
         partial);
   k_stats_final<<<1, 256, 0, lat->stream>>>(partial, nblocks, lat->err, fin);
   CUDA_TRY(cudaGetLastError(), "stats launch");
-  double h[ST_COUNT + 1];
-  CUDA_TRY(cudaMemcpyAsync(h, fin, sizeof h, cudaMemcpyDeviceToHost, lat->stream),
+  CUDA_TRY(cudaMemcpyAsync(h, fin, (ST_COUNT + 1) * sizeof(double),
+                           cudaMemcpyDeviceToHost, lat->stream),
            "stats copy");
-  CUDA_TRY(cudaStreamSynchronize(lat->stream), "stats");
+  return MLBM_OK;
+}
+
+mlbm_status stats_convert(mlbm_lattice* lat, const double* h, mlbm_stats* out) {
   // the error flag came back with the statistics
   if (h[ST_COUNT] != 0.0)
     if (mlbm_status st = check_device_error(lat)) return st;
@@ -723,6 +734,31 @@ mlbm_status mlbm_phase_stats(mlbm_lattice* lat, mlbm_stats* out) {
   out->min_p = h[ST_MINP];
   out->max_p = h[ST_MAXP];
   return MLBM_OK;
+}
+
+static_assert(ST_COUNT + 1 == MLBM_STATS_RAW_LEN, "raw statistics length");
+
+}  // namespace
+
+extern "C" {
+
+mlbm_status mlbm_phase_stats(mlbm_lattice* lat, mlbm_stats* out) {
+  if (!out) return fail(MLBM_ERR_ARG, "null output");
+  double h[ST_COUNT + 1];
+  if (mlbm_status st = stats_enqueue(lat, h)) return st;
+  CUDA_TRY(cudaStreamSynchronize(lat->stream), "stats");
+  return stats_convert(lat, h, out);
+}
+
+mlbm_status mlbm_phase_stats_async(mlbm_lattice* lat, double* raw) {
+  return stats_enqueue(lat, raw);
+}
+
+mlbm_status mlbm_stats_from_raw(mlbm_lattice* lat, const double* raw,
+                                mlbm_stats* out) {
+  if (mlbm_status st = check_lat(lat)) return st;
+  if (!raw || !out) return fail(MLBM_ERR_ARG, "null argument");
+  return stats_convert(lat, raw, out);
 }
 
 mlbm_status mlbm_plane_profile(mlbm_lattice* lat, int64_t* n_fluid_x,

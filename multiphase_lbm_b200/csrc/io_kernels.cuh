@@ -148,14 +148,17 @@ __global__ void __launch_bounds__(kStatThreads)
       acc[ST_RL] += (double)r;
       Nbr a;
       a.init(g, x, y, z);
-      uint32_t solid = 0u, other = 0u;
+      // all 18 neighbour densities as independent loads (every periodic
+      // index lies inside the array, solid nodes included), then the masks:
+      // a load under each direction's branch would wait on the one before
+      R nr[Q];
 #pragma unroll
-      for (int i = 1; i < Q; ++i) {
-        if (!((nb >> i) & 1u))
-          solid |= 1u << i;
-        else if (__ldg(rho + a.idx(-ex(i), -ey(i), -ez(i))) < rhol)
-          other |= 1u << i;
-      }
+      for (int i = 1; i < Q; ++i) nr[i] = __ldg(rho + a.idx(-ex(i), -ey(i), -ez(i)));
+      const uint32_t solid = ~nb & 0x7fffeu;  // directions 1..18
+      uint32_t low = 0u;
+#pragma unroll
+      for (int i = 1; i < Q; ++i) low |= (nr[i] < rhol ? 1u : 0u) << i;
+      const uint32_t other = low & nb & 0x7fffeu;
       const uint32_t first = (solid | other) & (0u - (solid | other));
       if (first & solid) acc[ST_NLS] += 1.0;
       else if (first) acc[ST_NLV] += 1.0;

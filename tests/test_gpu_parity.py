@@ -195,6 +195,34 @@ def test_phase_stats_match_oracle():
     assert abs(s["max_rho"] - o[9]) <= 1e-5 * abs(o[9])
 
 
+def test_async_stats_equal_sync_stats_every_step():
+    """mlbm_phase_stats_async, read one step later while the next step runs,
+    gives exactly the statistics mlbm_phase_stats gives at that step."""
+    import torch
+
+    from multiphase_lbm_b200 import capi
+    shape = (48, 40, 32)
+    fluid, rho = sphere_case(shape, seed=6, rho0=0.7, amp=0.05)
+    a, _ = _pair(shape, fluid, rho, **SC_PARAMS)
+    b, _ = _pair(shape, fluid, rho, **SC_PARAMS)
+    raw = [torch.zeros(capi.STATS_RAW_LEN, dtype=torch.float64).pin_memory().numpy()
+           for _ in range(2)]
+    ev = [torch.cuda.Event() for _ in range(2)]
+    got, want = [], []
+    for k in range(12):
+        a.iterate(k, 1)
+        a.stats_async(raw[k % 2])
+        ev[k % 2].record()
+        if k > 0:
+            ev[(k - 1) % 2].synchronize()
+            got.append(a.stats_from_raw(raw[(k - 1) % 2]))
+        b.iterate(k, 1)
+        want.append(b.stats())
+    ev[11 % 2].synchronize()
+    got.append(a.stats_from_raw(raw[11 % 2]))
+    assert got == want
+
+
 def test_mass_conservation_periodic_full_size():
     """Periodic, no injection: total fluid mass is conserved (BGK and
     bounce-back conserve mass); FP64 reduction, 200^3, 20 steps."""
