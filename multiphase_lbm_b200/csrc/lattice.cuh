@@ -215,7 +215,7 @@ __device__ __forceinline__ R psi_of(const Phys& p, R rho) {
 }
 
 // 0: interior fluid node, 1: inlet slab, 2: outlet slab (drainage boundary,
-// held at fixed density; absent from the reference, defined by this build).
+// held at fixed density; absent from the reference, defined by this library).
 __device__ __forceinline__ int bc_kind(const Phys& p, const Geom& g, int x) {
   return x < p.inlet_width ? 1 : (x >= g.lx - p.outlet_width ? 2 : 0);
 }

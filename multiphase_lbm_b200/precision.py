@@ -7,7 +7,7 @@ Reported for each storage format, at the end of the run:
   * saturation_error  |S - S_64| (S = liquid fluid nodes / fluid nodes);
   * interface_error   |x_if - x_if_64|, where x_if is the first x-plane at or
                       after the inlet slab whose liquid fraction over fluid
-                      nodes is >= 0.5 (a definition of this build: the
+                      nodes is >= 0.5 (a definition of this library: the
                       reference has no interface metric);
   * mass_drift        (M_end - M_0) / M_0 with M = sum of rho over fluid
                       nodes, accumulated in FP64 on the device;

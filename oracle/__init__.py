@@ -1,8 +1,9 @@
-"""The oracle: CPU checkers for the D3Q19 Shan-Chen time step.
+"""The oracle: CPU restatements of the D3Q19 Shan-Chen time step that the
+tests compare the library against.
 
 TEST INFRASTRUCTURE ONLY.  Imported by ``tests/``, ``__graft_entry__.smoke()``
-and the ``cpu_baseline`` / ``--impl reference`` legs of ``bench.py`` -- as the
-checker or the timed CPU baseline, never by the product library.
+and the ``cpu_baseline`` / ``--impl reference`` legs of ``bench.py`` -- to
+verify results or as the timed CPU baseline, never by the product library.
 
 Two implementations, both on the reference layout (scalars ``[x][y][z]`` with
 z fastest, populations ``[x][y][z][19]``):

@@ -1,7 +1,7 @@
 /*
  * mlbm_oracle.c -- TEST INFRASTRUCTURE ONLY (the oracle).  Never linked into
  * or called by the product; only tests/, __graft_entry__.smoke() and the
- * cpu_baseline leg of bench.py use it, as the checker.
+ * cpu_baseline leg of bench.py use it, to verify results.
  *
  * A plain-C restatement, with runtime lattice sizes, of the reference's D3Q19
  * single-component Shan-Chen time step (Amber1995/multiphase_LBM):

@@ -1,6 +1,6 @@
 """Shared fixtures.  ``-m gpu`` tests need a CUDA device; everything else runs
-on the CPU.  Native libraries are built in-tree on first use (the GPU box
-receives them prebuilt)."""
+on the CPU.  Native libraries are built in-tree on first use (a machine that
+receives the tree with them built uses them as they are)."""
 import os
 import sys
 
