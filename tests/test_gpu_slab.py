@@ -99,3 +99,12 @@ def test_slab_refuses_whole_lattice_calls():
     finally:
         for s in run.slabs:
             s.close()
+
+
+@pytest.mark.parametrize("storage_name,steps", [("STORE_F32", 101), ("STORE_F16", 50)])
+def test_long_run_four_slabs(storage_name, steps):
+    """Many steps through both AA phases: the decomposition stays bit for bit
+    on the whole lattice's trajectory (drainage boundary, 64^3)."""
+    from multiphase_lbm_b200 import capi
+    _compare((64, 64, 64), 4, getattr(capi, storage_name), steps, DRAIN,
+             seed=17)
