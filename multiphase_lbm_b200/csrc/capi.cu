@@ -671,9 +671,15 @@ mlbm_status stats_enqueue(mlbm_lattice* lat, double* h) {
                 "phase statistics of a slab would count its halo planes: "
                 "gather the slabs' own planes first");
   if (mlbm_status st = activate(lat)) return st;
+  // a lattice held in the fluid-only layout is walked through its node
+  // table (no lanes idle on solid nodes); otherwise the dense grid
+  const CompactState& c = lat->compact;
+  const bool fluid_list = c.active && c.cinfo && lat->storage != MLBM_STORE_F64;
   const dim3 grid(lat->g.px / 32, (lat->g.ly + 7) / 8,
                   (lat->g.lz + kStatZ - 1) / kStatZ);
-  const long long nblocks = (long long)grid.x * grid.y * grid.z;
+  const long long nblocks = fluid_list
+                                ? (c.nfluid + kStatSlots - 1) / kStatSlots
+                                : (long long)grid.x * grid.y * grid.z;
   const size_t need = ((size_t)nblocks + 1) * ST_COUNT * sizeof(double) + sizeof(double);
   if (lat->stats_scratch_bytes < need) {
     // a larger area: earlier calls may still be reading the old one
@@ -686,7 +692,12 @@ mlbm_status stats_enqueue(mlbm_lattice* lat, double* h) {
   }
   double* partial = lat->stats_scratch;
   double* fin = partial + (size_t)nblocks * ST_COUNT;
-  if (lat->storage == MLBM_STORE_F64)
+  if (fluid_list) {
+    if (nblocks > 0)
+      k_stats_fluid<float><<<(unsigned)nblocks, kStatThreads, 0, lat->stream>>>(
+          static_cast<const float*>(lat->rho), c.cinfo, c.nfluid, lat->g,
+          lat->phys, partial);
+  } else if (lat->storage == MLBM_STORE_F64)
     k_stats_partial<double><<<grid, dim3(32, 8), 0, lat->stream>>>(
         static_cast<const double*>(lat->rho), lat->nbw, lat->g, lat->phys,
         partial);

@@ -122,11 +122,76 @@ __device__ __forceinline__ double stat_identity(int k) {
                                            : 0.0;
 }
 
-// One block per 32 x 8 nodes of an (x, y) plane and kStatZ planes; partial
-// sums per block, reduced in a fixed order (deterministic).  The liquid
-// boundary test reads the node's neighbour word (bit i: x - e_i is fluid) and
-// the density of every fluid neighbour, then takes the first neighbour
+// The statistics of one fluid node folded into acc.  The liquid boundary
+// test reads the node's neighbour word (bit i: x - e_i is fluid) and the
+// density of every fluid neighbour, then takes the first neighbour
 // (i = 1..18) that is solid or not liquid, as calc_cluster does.
+template <typename R>
+__device__ __forceinline__ void stat_node(double (&acc)[ST_COUNT],
+                                          const R* __restrict__ rho,
+                                          const Geom& g, const Phys& p, int x,
+                                          int y, int z, uint32_t nb, R r) {
+  const R rhol = R(p.rhol_spinodal), rhog = R(p.rhog_spinodal);
+  const R pr = pressure_of<R>(p, r);
+  acc[ST_NF] += 1.0;
+  acc[ST_MASS] += (double)r;
+  if (r > rhol) {
+    acc[ST_NL] += 1.0;
+    acc[ST_PL] += (double)pr;
+    acc[ST_RL] += (double)r;
+    Nbr a;
+    a.init(g, x, y, z);
+    // all 18 neighbour densities as independent loads (every periodic
+    // index lies inside the array, solid nodes included), then the masks:
+    // a load under each direction's branch would wait on the one before
+    R nr[Q];
+#pragma unroll
+    for (int i = 1; i < Q; ++i) nr[i] = __ldg(rho + a.idx(-ex(i), -ey(i), -ez(i)));
+    const uint32_t solid = ~nb & 0x7fffeu;  // directions 1..18
+    uint32_t low = 0u;
+#pragma unroll
+    for (int i = 1; i < Q; ++i) low |= (nr[i] < rhol ? 1u : 0u) << i;
+    const uint32_t other = low & nb & 0x7fffeu;
+    const uint32_t first = (solid | other) & (0u - (solid | other));
+    if (first & solid) acc[ST_NLS] += 1.0;
+    else if (first) acc[ST_NLV] += 1.0;
+  } else if (r < rhog) {
+    acc[ST_NV] += 1.0;
+    acc[ST_PV] += (double)pr;
+    acc[ST_RV] += (double)r;
+  }
+  acc[ST_MINR] = fmin(acc[ST_MINR], (double)r);
+  acc[ST_MAXR] = fmax(acc[ST_MAXR], (double)r);
+  acc[ST_MINP] = fmin(acc[ST_MINP], (double)pr);
+  acc[ST_MAXP] = fmax(acc[ST_MAXP], (double)pr);
+}
+
+// Warp then block reduction of acc in a fixed order (deterministic); thread 0
+// .. ST_COUNT - 1 of the block write the block's record.  256 threads.
+__device__ __forceinline__ void stat_block_reduce(double (&acc)[ST_COUNT],
+                                                  int tid, double* record) {
+#pragma unroll
+  for (int k = 0; k < ST_COUNT; ++k) {
+    double v = acc[k];
+    for (int off = 16; off > 0; off >>= 1)
+      v = stat_op(k, v, __shfl_down_sync(0xffffffffu, v, off));
+    acc[k] = v;
+  }
+  __shared__ double sh[kStatThreads / 32][ST_COUNT];
+  const int warp = tid >> 5, lane = tid & 31;
+  if (lane == 0)
+    for (int k = 0; k < ST_COUNT; ++k) sh[warp][k] = acc[k];
+  __syncthreads();
+  if (tid < ST_COUNT) {
+    const int k = tid;
+    double v = sh[0][k];
+    for (int w = 1; w < kStatThreads / 32; ++w) v = stat_op(k, v, sh[w][k]);
+    record[k] = v;
+  }
+}
+
+// Dense form: one block per 32 x 8 nodes of an (x, y) plane and kStatZ
+// planes; each thread folds its column of nodes, z ascending.
 template <typename R>
 __global__ void __launch_bounds__(kStatThreads)
     k_stats_partial(const R* __restrict__ rho, const uint32_t* __restrict__ nbw,
@@ -137,41 +202,6 @@ __global__ void __launch_bounds__(kStatThreads)
   const int x = blockIdx.x * 32 + threadIdx.x;
   const int y = blockIdx.y * blockDim.y + threadIdx.y;
   const int z0 = blockIdx.z * kStatZ, z1 = min(z0 + kStatZ, g.lz);
-  const R rhol = R(p.rhol_spinodal), rhog = R(p.rhog_spinodal);
-  auto node = [&](int z, uint32_t nb, R r) {
-    const R pr = pressure_of<R>(p, r);
-    acc[ST_NF] += 1.0;
-    acc[ST_MASS] += (double)r;
-    if (r > rhol) {
-      acc[ST_NL] += 1.0;
-      acc[ST_PL] += (double)pr;
-      acc[ST_RL] += (double)r;
-      Nbr a;
-      a.init(g, x, y, z);
-      // all 18 neighbour densities as independent loads (every periodic
-      // index lies inside the array, solid nodes included), then the masks:
-      // a load under each direction's branch would wait on the one before
-      R nr[Q];
-#pragma unroll
-      for (int i = 1; i < Q; ++i) nr[i] = __ldg(rho + a.idx(-ex(i), -ey(i), -ez(i)));
-      const uint32_t solid = ~nb & 0x7fffeu;  // directions 1..18
-      uint32_t low = 0u;
-#pragma unroll
-      for (int i = 1; i < Q; ++i) low |= (nr[i] < rhol ? 1u : 0u) << i;
-      const uint32_t other = low & nb & 0x7fffeu;
-      const uint32_t first = (solid | other) & (0u - (solid | other));
-      if (first & solid) acc[ST_NLS] += 1.0;
-      else if (first) acc[ST_NLV] += 1.0;
-    } else if (r < rhog) {
-      acc[ST_NV] += 1.0;
-      acc[ST_PV] += (double)pr;
-      acc[ST_RV] += (double)r;
-    }
-    acc[ST_MINR] = fmin(acc[ST_MINR], (double)r);
-    acc[ST_MAXR] = fmax(acc[ST_MAXR], (double)r);
-    acc[ST_MINP] = fmin(acc[ST_MINP], (double)pr);
-    acc[ST_MAXP] = fmax(acc[ST_MAXP], (double)pr);
-  };
   if (x < g.lx && y < g.ly) {
     // eight planes' node words and densities in flight at once (4: 1 %
     // slower end to end; 8 planes per block with more blocks: 5 % slower)
@@ -192,31 +222,55 @@ __global__ void __launch_bounds__(kStatThreads)
       }
 #pragma unroll
       for (int j = 0; j < U; ++j)
-        if (nbv[j] & NB_SELF) node(zb + j, nbv[j], rv[j]);
+        if (nbv[j] & NB_SELF) stat_node<R>(acc, rho, g, p, x, y, zb + j, nbv[j], rv[j]);
     }
   }
-  // warp then block reduction in a fixed order (deterministic)
+  const long long blk =
+      blockIdx.x + (long long)gridDim.x * (blockIdx.y + (long long)gridDim.y * blockIdx.z);
+  stat_block_reduce(acc, threadIdx.y * 32 + threadIdx.x, partial + blk * ST_COUNT);
+}
+
+// Fluid-list form, for a lattice held in the fluid-only layout: the threads
+// walk the compact node table (node word, packed x, y, z), so no lane idles
+// on a solid node.  Block b folds slots [b * kStatSlots, (b + 1) *
+// kStatSlots); thread t takes slots t, t + 256, ... of them, ascending.
+constexpr int kStatSlotsPerThread = 16;
+constexpr int kStatSlots = kStatThreads * kStatSlotsPerThread;
+
+template <typename R>
+__global__ void __launch_bounds__(kStatThreads)
+    k_stats_fluid(const R* __restrict__ rho, const uint2* __restrict__ cinfo,
+                  long long nslots, Geom g, Phys p, double* __restrict__ partial) {
+  double acc[ST_COUNT];
 #pragma unroll
-  for (int k = 0; k < ST_COUNT; ++k) {
-    double v = acc[k];
-    for (int off = 16; off > 0; off >>= 1)
-      v = stat_op(k, v, __shfl_down_sync(0xffffffffu, v, off));
-    acc[k] = v;
+  for (int k = 0; k < ST_COUNT; ++k) acc[k] = stat_identity(k);
+  const long long base = (long long)blockIdx.x * kStatSlots + threadIdx.x;
+  constexpr int U = 8;
+#pragma unroll 1
+  for (int j0 = 0; j0 < kStatSlotsPerThread; j0 += U) {
+    uint2 ci[U];
+    R rv[U];
+#pragma unroll
+    for (int j = 0; j < U; ++j) {
+      const long long k = base + (long long)(j0 + j) * kStatThreads;
+      ci[j] = k < nslots ? __ldg(cinfo + k) : make_uint2(0u, 0u);
+    }
+#pragma unroll
+    for (int j = 0; j < U; ++j) {
+      rv[j] = R(0);
+      if (ci[j].x & NB_SELF)
+        rv[j] = __ldg(rho + node_index(g, (int)(ci[j].y & 2047u),
+                                       (int)((ci[j].y >> 11) & 2047u),
+                                       (int)(ci[j].y >> 22)));
+    }
+#pragma unroll
+    for (int j = 0; j < U; ++j)
+      if (ci[j].x & NB_SELF)
+        stat_node<R>(acc, rho, g, p, (int)(ci[j].y & 2047u),
+                     (int)((ci[j].y >> 11) & 2047u), (int)(ci[j].y >> 22),
+                     ci[j].x, rv[j]);
   }
-  __shared__ double sh[kStatThreads / 32][ST_COUNT];
-  const int tid = threadIdx.y * 32 + threadIdx.x;
-  const int warp = tid >> 5, lane = tid & 31;
-  if (lane == 0)
-    for (int k = 0; k < ST_COUNT; ++k) sh[warp][k] = acc[k];
-  __syncthreads();
-  if (tid < ST_COUNT) {
-    const int k = tid;
-    double v = sh[0][k];
-    for (int w = 1; w < kStatThreads / 32; ++w) v = stat_op(k, v, sh[w][k]);
-    const long long blk =
-        blockIdx.x + (long long)gridDim.x * (blockIdx.y + (long long)gridDim.y * blockIdx.z);
-    partial[blk * ST_COUNT + k] = v;
-  }
+  stat_block_reduce(acc, threadIdx.x, partial + (long long)blockIdx.x * ST_COUNT);
 }
 
 // Reduce the per-block partials (fixed-order tree: deterministic) and append
