@@ -15,7 +15,9 @@ and compiles with g++:
   the reference host driver (src/multiphase_lbm.cu), run on the host through
   oracle/ref_shim.h and oracle/ref_harness.cpp (OpenMP over x);
 * ``oracle/_ref/multiphaselbm_cpu_<lx>x<ly>x<lz>`` -- the reference program
-  (src/main.cc) linked against the same objects.
+  (src/main.cc) linked against the same objects;
+* ``oracle/_ref/multiphaselbm_cuda_200x200x200`` -- the reference program
+  with its own CUDA kernels, built for sm_100a (timing only).
 
 Run: ``python oracle/build_ref.py [--sizes 16x12x10,64x64x64]``.  Without the
 reference sources present (as on a machine that only receives the built
@@ -159,6 +161,40 @@ def build_dropin(sizes=None, force: bool = False) -> list[str]:
     return out
 
 
+# The reference program as the reference builds it for the GPU (its own
+# kernels, src/iteration_host.cu), compiled for sm_100a: only to time the
+# reference's CUDA path on the B200 beside this library.  Not a parity
+# oracle (its collision kernel reads neighbours another thread may be
+# writing, so its results are not deterministic).
+CUDA_SIZES = ["200x200x200"]
+
+
+def build_cuda(sizes=None, force: bool = False) -> list[str]:
+    """Build oracle/_ref/multiphaselbm_cuda_<size>."""
+    if not os.path.isdir(os.path.join(REFERENCE, "include")):
+        return []
+    nvcc = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+    scratch = os.path.join(tempfile.gettempdir(), "mlbm_ref_build")
+    os.makedirs(OUT, exist_ok=True)
+    out = []
+    for size in sizes or CUDA_SIZES:
+        exe = os.path.join(OUT, f"multiphaselbm_cuda_{size}")
+        if not force and os.path.exists(exe):
+            out.append(exe)
+            continue
+        root = _prepare_tree(size, scratch)
+        cmd = [nvcc, "-O3", "-std=c++14", "-w",
+               "-gencode", "arch=compute_100a,code=sm_100a",
+               "-I", os.path.join(root, "include"),
+               "-I", os.path.join(root, "external"),
+               os.path.join(root, "src", "iteration_host.cu"),
+               os.path.join(root, "src", "multiphase_lbm.cu"),
+               os.path.join(root, "src", "main.cc"), "-o", exe]
+        subprocess.run(cmd, check=True)
+        out.append(exe)
+    return out
+
+
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
     ap.add_argument("--sizes", default=",".join(SIZES))
@@ -166,6 +202,7 @@ def main(argv=None) -> int:
     args = ap.parse_args(argv)
     libs = build(args.sizes.split(","), force=args.force, quiet=False)
     libs += build_dropin(args.sizes.split(","), force=args.force)
+    libs += build_cuda(force=args.force)
     if not libs:
         print("reference sources not present; nothing built")
     return 0
