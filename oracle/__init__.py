@@ -66,7 +66,8 @@ def build() -> None:
     subprocess.run(["make", "-s", "-C", HERE], check=True)
     from . import build_ref  # noqa: WPS433
     build_ref.build()
-    build_ref.build_dropin(["40x40x40"])
+    build_ref.build_dropin(["40x40x40", "200x200x200"])
+    build_ref.build_cuda()  # the reference's CUDA program, timing only
 
 
 def _load(path: str) -> C.CDLL:

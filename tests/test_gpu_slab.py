@@ -108,3 +108,26 @@ def test_long_run_four_slabs(storage_name, steps):
     from multiphase_lbm_b200 import capi
     _compare((64, 64, 64), 4, getattr(capi, storage_name), steps, DRAIN,
              seed=17)
+
+
+def test_ring_refuses_slabs_of_different_lattices():
+    """A ring whose neighbouring halo and edge planes differ in size is
+    refused at creation (the kernel would copy past a plane)."""
+    from multiphase_lbm_b200 import capi, slab
+    fa, ra = sphere_case((32, 24, 20), seed=1, rmin=2.5, rmax=5.0,
+                         porosity=0.55, rho0=1.9, amp=0.05)
+    fb, rb = sphere_case((32, 24, 20), seed=2, rmin=2.5, rmax=5.0,
+                         porosity=0.55, rho0=1.9, amp=0.05)
+    p = capi.default_params(**DRAIN)
+    a = slab.Slab(fa, ra, p, 0, 10)
+    b = slab.Slab(fb, rb, p, 10, 10)
+    try:
+        with pytest.raises(capi.MlbmError, match="halo and edge"):
+            slab.RingExchange([a, b])
+        whole = _whole(capi, fa, ra, capi.STORE_F32, p)
+        with pytest.raises(capi.MlbmError, match="not a slab"):
+            whole.halo_segments(capi.HALO_POP_EDGE, 0)
+        whole.close()
+    finally:
+        a.close()
+        b.close()
