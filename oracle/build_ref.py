@@ -148,6 +148,7 @@ def build_dropin(sizes=None, force: bool = False) -> list[str]:
         with open(os.path.join(gen, "iteration_host.h"), "w") as fh:
             fh.write(COMPAT_HEADER)
         cmd = [nvcc, "-O2", "-std=c++14", "-w", "-Xcompiler", "-fopenmp",
+               "-gencode", "arch=compute_100a,code=sm_100a",
                "-I", gen, "-I", os.path.join(root, "include"),
                "-I", os.path.join(root, "external"),
                "-I", os.path.join(root_repo, "include"),
