@@ -200,3 +200,25 @@ def test_rank_moves_over_gloo_match_local_moves(world):
             assert res[r][0][key] == [t.tolist() for t in segs], (r, key)
         for key, segs in want_out[r].items():
             assert res[r][1][key] == [t.tolist() for t in segs], (r, key)
+
+
+def test_push_masks_match_brute_force():
+    """slab.push_masks against a direct walk of the plane: for each fluid node
+    of the edge plane in layout order (rows y, then x) and each direction s
+    crossing the face, whether the node y - e_s that would push into it is
+    fluid; a hole entry (False) pads an odd count."""
+    rng = np.random.default_rng(8)
+    f = (rng.random((7, 5, 6)) < 0.6).astype(np.uint8)
+    lx, ly, lz = f.shape
+    for side, dz in ((0, 1), (1, -1)):
+        z = 1 if side == 0 else lz - 2
+        got = slab.push_masks(f, side)
+        dirs = [d for d in range(1, 19) if slab._EZ[d] == dz]
+        nodes = [(x, y) for y in range(ly) for x in range(lx) if f[x, y, z]]
+        assert len(got) == len(dirs)
+        for m, d in zip(got, dirs):
+            want = [bool(f[(x - slab._EX[d]) % lx, (y - slab._EY[d]) % ly, z - dz])
+                    for x, y in nodes]
+            if len(want) % 2:
+                want.append(False)
+            assert m.tolist() == want
