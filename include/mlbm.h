@@ -340,7 +340,9 @@ mlbm_status mlbm_halo_segments(mlbm_lattice* lat, int32_t kind, int32_t side,
  * exchange waits for every slab's stream and every slab's stream waits for
  * it.  what: MLBM_RING_POP_IN (before an AA phase-0 step), MLBM_RING_PSI
  * (between the passes), MLBM_RING_POP_OUT (after a phase-0 update; merges
- * each received slot only where its pusher is fluid). */
+ * each received slot only where its pusher is fluid).  The ring holds raw
+ * device addresses of its slabs: destroy it before any of them, and build a
+ * new one after a slab's mask changes. */
 typedef struct mlbm_slab_ring mlbm_slab_ring;
 #define MLBM_RING_POP_IN 0
 #define MLBM_RING_PSI 1

@@ -345,6 +345,15 @@ class SlabRun:
         for s in range(nsteps):
             self.step(step0 + s, **kw)
 
+    def close(self) -> None:
+        """Release the transport, then the slabs (a ring holds their device
+        addresses, so it goes first)."""
+        close = getattr(self.exchange, "close", None)
+        if close:
+            close()
+        for s in self.slabs:
+            s.close()
+
 
 def decompose(fluid: np.ndarray, rho: np.ndarray, params, parts: int,
               storage: int = capi.STORE_F32,

@@ -47,8 +47,7 @@ def _compare(shape, parts, storage, steps, params_kw, seed=5, transport="ring"):
             b = slab.gather(run.slabs, which)
             assert np.array_equal(a[m], b[m]), (which, shape, parts, steps)
     finally:
-        for s in run.slabs:
-            s.close()
+        run.close()
         whole.close()
 
 
@@ -97,8 +96,7 @@ def test_slab_refuses_whole_lattice_calls():
         with pytest.raises(capi.MlbmError):
             lat.step_pass(0, 2)
     finally:
-        for s in run.slabs:
-            s.close()
+        run.close()
 
 
 @pytest.mark.parametrize("storage_name,steps", [("STORE_F32", 101), ("STORE_F16", 50)])
