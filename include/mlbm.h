@@ -193,6 +193,16 @@ mlbm_status mlbm_iterate(mlbm_lattice* lat, int64_t step0, int32_t nsteps,
  *                the update tiles (a wavefront along z), so the update reads
  *                the populations back from L2 and DRAM sees them once per
  *                step.  Bit-identical to TWO_PASS; same limits as COMPACT;
+ *   BAND         ONE launch per step over the fluid-only layout with two
+ *                population buffers: the launch reads the step's
+ *                populations from one buffer and pushes the new ones into
+ *                the other, so no block waits for another; a block forms
+ *                psi of a band of rows (plus one halo row on either side) in
+ *                shared memory plane by plane and updates the band one plane
+ *                behind, so DRAM sees the populations once per step.
+ *                Bit-identical to TWO_PASS; FP32 / FP16 storage, whole
+ *                lattices (not slabs), same size limits as COMPACT; a
+ *                second population buffer is allocated on first use;
  *   AUTO         (default) COMPACT where supported, else TWO_PASS.
  * The state moves between the layouts on demand (the dense buffers stay
  * allocated; the fluid-only layout adds 19 populations and 14 words per
@@ -203,6 +213,7 @@ mlbm_status mlbm_iterate(mlbm_lattice* lat, int64_t step0, int32_t nsteps,
 #define MLBM_KERNEL_COMPACT 3
 #define MLBM_KERNEL_SINGLE_PASS 4
 #define MLBM_KERNEL_WAVE 5
+#define MLBM_KERNEL_BAND 6
 mlbm_status mlbm_set_step_kernel(mlbm_lattice* lat, int32_t kind);
 /* The kernel the next mlbm_iterate runs (AUTO resolved); -1 for NULL. */
 int32_t mlbm_get_step_kernel(const mlbm_lattice* lat);
@@ -211,6 +222,12 @@ int32_t mlbm_get_step_kernel(const mlbm_lattice* lat);
  * planes (0..256, default 4). */
 mlbm_status mlbm_set_wave_shape(mlbm_lattice* lat, int32_t tile_nodes,
                                 int32_t lookahead);
+/* Tiling of the BAND step: bands of about `rows` rows (y, 1..64) and chunks
+ * of about `planes` planes (z, 1..1024), one block per band and chunk.
+ * Default 4 x 24.  MLBM_ERR_ARG when a band's psi planes do not fit shared
+ * memory (4 x (rows + 2) x (lx + 2) floats). */
+mlbm_status mlbm_set_band_shape(mlbm_lattice* lat, int32_t rows,
+                                int32_t planes);
 /* Tiling of the SINGLE_PASS step: a block walks `rows` full x-rows (y) through
  * `planes` planes (z); at least two tiles along y and z, each at least two
  * rows / planes deep.  Default 4 x 8. */

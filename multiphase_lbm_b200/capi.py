@@ -24,7 +24,7 @@ HALO_PSI_EDGE, HALO_PSI_GHOST, HALO_POP_EDGE, HALO_POP_GHOST = 0, 1, 2, 3
 HALO_MAX_SEGMENTS = 5
 STATS_RAW_LEN = 15
 (KERNEL_AUTO, KERNEL_FUSED, KERNEL_TWO_PASS, KERNEL_COMPACT,
- KERNEL_SINGLE_PASS, KERNEL_WAVE) = 0, 1, 2, 3, 4, 5
+ KERNEL_SINGLE_PASS, KERNEL_WAVE, KERNEL_BAND) = 0, 1, 2, 3, 4, 5, 6
 Q = 19
 
 STATUS = {0: "MLBM_OK", 1: "MLBM_ERR_ARG", 2: "MLBM_ERR_CUDA",
@@ -118,6 +118,7 @@ SIGNATURES = [
     ("mlbm_set_update_shape", C.c_int, [_VP, C.c_int32, C.c_int32]),
     ("mlbm_set_compact_shape", C.c_int, [_VP, C.c_int32, C.c_int32]),
     ("mlbm_set_wave_shape", C.c_int, [_VP, C.c_int32, C.c_int32]),
+    ("mlbm_set_band_shape", C.c_int, [_VP, C.c_int32, C.c_int32]),
     ("mlbm_get_step_kernel", C.c_int32, [_VP]),
     ("mlbm_autotune", C.c_int, [_VP, C.c_int64, C.c_int32, _VP, _VP]),
     ("mlbm_set_slab", C.c_int, [_VP, C.c_int32]),
@@ -221,6 +222,10 @@ class Lattice:
         """Work items of the wavefront step: fluid nodes per item and the
         lead of the density tiles over the update tiles, in planes."""
         check(lib().mlbm_set_wave_shape(self.h, tile_nodes, lookahead))
+
+    def set_band_shape(self, rows: int = 4, planes: int = 24) -> None:
+        """Tiling of KERNEL_BAND: rows per band (y) and planes per chunk (z)."""
+        check(lib().mlbm_set_band_shape(self.h, rows, planes))
 
     def set_compact_shape(self, rows: int = 4, planes: int = 8) -> None:
         """Tiling of the single-pass step (rows along y, planes along z)."""

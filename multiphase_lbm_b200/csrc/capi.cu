@@ -220,12 +220,13 @@ mlbm_status launch_steps(mlbm_lattice* lat, int64_t step0, int32_t nsteps,
   const bool fused = kind == MLBM_KERNEL_FUSED && lat->fused.ok;
   if (kind == MLBM_KERNEL_FUSED && !lat->fused.ok)
     return fail(MLBM_ERR_ARG, "fused kernel does not fit this lattice");
-  bool compact = false, single = false, wave = false;
+  bool compact = false, single = false, wave = false, band = false;
   if constexpr (!std::is_same<T, double>::value) {
     compact = kind == MLBM_KERNEL_COMPACT || kind == MLBM_KERNEL_SINGLE_PASS ||
-              kind == MLBM_KERNEL_WAVE;
+              kind == MLBM_KERNEL_WAVE || kind == MLBM_KERNEL_BAND;
     single = kind == MLBM_KERNEL_SINGLE_PASS;
     wave = kind == MLBM_KERNEL_WAVE;
+    band = kind == MLBM_KERNEL_BAND;
   }
   if ((flags & MLBM_ITER_WRITE_VELOCITY) && !lat->vel) {
     // the velocity field is allocated on first request
@@ -251,9 +252,13 @@ mlbm_status launch_steps(mlbm_lattice* lat, int64_t step0, int32_t nsteps,
     const bool wu = (flags & MLBM_ITER_WRITE_VELOCITY) && last;
     const int out = wu ? (OUT_RHO | OUT_VEL) : (last ? OUT_RHO : OUT_NONE);
     mlbm_status st;
+    // the one-pass step starts and ends in AA phase 1; from phase 0 one
+    // two-pass step gets there
+    const bool one_pass = band && lat->phase == 1;
     if constexpr (!std::is_same<T, double>::value) {
       if (single) st = launch_compact<T>(lat, a, out);
       else if (wave) st = launch_compact_wave<T>(lat, a, wu, last);
+      else if (one_pass) st = launch_compact_band<T>(lat, a, wu, last);
       else if (compact) st = launch_compact_two_pass<T>(lat, a, wu, last);
       else if (fused) st = launch_fused<T>(lat, a, out);
       else st = launch_two_pass<T>(lat, a, wu, last);
@@ -263,7 +268,7 @@ mlbm_status launch_steps(mlbm_lattice* lat, int64_t step0, int32_t nsteps,
       else st = launch_two_pass<T>(lat, a, wu, last);
     }
     if (st) return st;
-    lat->phase ^= 1;
+    if (!one_pass) lat->phase ^= 1;
     if (wu) lat->vel_valid = true;
   }
   return MLBM_OK;
@@ -801,8 +806,14 @@ mlbm_status mlbm_plane_profile(mlbm_lattice* lat, int64_t* n_fluid_x,
 
 mlbm_status mlbm_set_step_kernel(mlbm_lattice* lat, int32_t kind) {
   if (mlbm_status st = check_lat(lat)) return st;
-  if (kind < MLBM_KERNEL_AUTO || kind > MLBM_KERNEL_WAVE)
+  if (kind < MLBM_KERNEL_AUTO || kind > MLBM_KERNEL_BAND)
     return fail(MLBM_ERR_ARG, "invalid step kernel %d", kind);
+  if (kind == MLBM_KERNEL_BAND &&
+      !compact_band_supported(lat, lat->compact.band_rows))
+    return fail(MLBM_ERR_ARG,
+                "one-pass step needs FP32 or FP16 storage, at most 2048 x 2048 "
+                "x 1024 nodes, a whole lattice (not a slab) and bands that "
+                "fit shared memory");
   if (kind == MLBM_KERNEL_FUSED && !lat->fused.ok)
     return fail(MLBM_ERR_ARG, "fused kernel does not fit this lattice");
   if ((kind == MLBM_KERNEL_COMPACT || kind == MLBM_KERNEL_WAVE) &&
@@ -846,6 +857,15 @@ mlbm_status mlbm_set_update_shape(mlbm_lattice* lat, int32_t rows,
 
 int32_t mlbm_get_step_kernel(const mlbm_lattice* lat) {
   return lat ? effective_kernel(lat) : -1;
+}
+
+mlbm_status mlbm_set_band_shape(mlbm_lattice* lat, int32_t rows,
+                                int32_t planes) {
+  if (mlbm_status st = check_lat(lat)) return st;
+  if (rows < 1 || rows > 64 || planes < 1 || planes > 1024)
+    return fail(MLBM_ERR_ARG, "invalid one-pass shape %d rows x %d planes",
+                rows, planes);
+  return compact_set_band_shape(lat, rows, planes);
 }
 
 mlbm_status mlbm_set_wave_shape(mlbm_lattice* lat, int32_t tile_nodes,

@@ -51,6 +51,9 @@ struct CompactState {
   int wave_par = 0;                    // counter set of the next launch
   int wave_grid[2] = {0, 0};           // persistent CTAs per AA phase
   bool wave_built = false;             // work list matches tables and shape
+  // one-pass step (band.cuh): the second population buffer and the tiling
+  void* cpop_alt = nullptr;            // [Q][cs] populations (T)
+  int band_rows = 4, band_planes = 24;  // requested rows per band, planes per chunk
 };
 }  // namespace mlbm
 
@@ -129,4 +132,11 @@ mlbm_status launch_compact_wave(mlbm_lattice* lat, const StepArgs& a,
                                 bool write_u, bool write_rho);
 mlbm_status compact_set_wave_shape(mlbm_lattice* lat, int tile, int lookahead);
 void compact_reset_wave(mlbm_lattice* lat);  // after a failed wait
+// One-pass step over the compact layout with two buffers (compact.cu,
+// band.cuh); starts and ends in AA phase 1.
+template <typename T>
+mlbm_status launch_compact_band(mlbm_lattice* lat, const StepArgs& a,
+                                bool write_u, bool write_rho);
+bool compact_band_supported(const mlbm_lattice* lat, int rows);
+mlbm_status compact_set_band_shape(mlbm_lattice* lat, int rows, int planes);
 }  // namespace mlbm

@@ -9,6 +9,7 @@
 
 #include "capi_internal.h"
 #include "compact.cuh"
+#include "band.cuh"
 #include "compact2.cuh"
 #include "wave.cuh"
 
@@ -139,6 +140,8 @@ mlbm_status build_tables(mlbm_lattice* lat) {
   c.cs = std::max(64LL, (c.nfluid + 63) / 64 * 64);
   if (c.cs > c.cap) {
     cudaFree(c.cpop);
+    cudaFree(c.cpop_alt);
+    c.cpop_alt = nullptr;
     cudaFree(c.part);
     cudaFree(c.cnb);
     cudaFree(c.cinfo);
@@ -321,6 +324,7 @@ void compact_invalidate(mlbm_lattice* lat) {
 void compact_free(mlbm_lattice* lat) {
   CompactState& c = lat->compact;
   cudaFree(c.cpop);
+  cudaFree(c.cpop_alt);
   cudaFree(c.part);
   cudaFree(c.cnb);
   cudaFree(c.cinfo);
@@ -645,5 +649,112 @@ mlbm_status launch_compact_wave(mlbm_lattice* lat, const StepArgs& a,
 
 template mlbm_status launch_compact_wave<float>(mlbm_lattice*, const StepArgs&, bool, bool);
 template mlbm_status launch_compact_wave<__half>(mlbm_lattice*, const StepArgs&, bool, bool);
+
+// ---- one-pass step (band.cuh) ---------------------------------------------------
+
+namespace {
+
+constexpr size_t kBandSmemMax = 227 * 1024;
+
+// Bands of about `rows` rows along y and chunks of about `planes` planes
+// along z; the tallest band's psi ring must fit shared memory.
+BandShape band_shape(const Geom& g, int rows, int planes) {
+  BandShape s;
+  s.nb = std::max(1, g.ly / std::max(1, rows));
+  s.nc = std::max(1, g.lz / std::max(1, planes));
+  s.hmax = (g.ly + s.nb - 1) / s.nb;
+  return s;
+}
+
+template <typename T, bool WR, bool WU>
+const void* band_fn() {
+  return reinterpret_cast<const void*>(&k_band<T, WR, WU>);
+}
+
+template <typename T>
+const void* pick_band(bool wr, bool wu) {
+  if (wu) return band_fn<T, true, true>();
+  return wr ? band_fn<T, true, false>() : band_fn<T, false, false>();
+}
+
+// The dynamic shared-memory limit is an attribute of the kernel on each
+// device: raise it (never lower it) to the largest size any lattice needs.
+template <typename T>
+mlbm_status band_smem_attr(int device, size_t smem) {
+  static std::mutex mu;
+  static size_t done[64] = {};
+  std::lock_guard<std::mutex> lock(mu);
+  if (device >= 0 && device < 64 && done[device] >= smem) return MLBM_OK;
+  for (int v = 0; v < 3; ++v) {
+    const cudaError_t e = cudaFuncSetAttribute(
+        pick_band<T>(v >= 1, v == 2), cudaFuncAttributeMaxDynamicSharedMemorySize,
+        (int)smem);
+    if (e != cudaSuccess) return cuda_fail(e, "one-pass step attribute");
+  }
+  if (device >= 0 && device < 64) done[device] = smem;
+  return MLBM_OK;
+}
+
+}  // namespace
+
+bool compact_band_supported(const mlbm_lattice* lat, int rows) {
+  if (!lat->compact.two_pass_ok || lat->slab) return false;
+  const BandShape s = band_shape(lat->g, rows, 1);
+  return band_smem_bytes(s.hmax, lat->g.lx) <= kBandSmemMax;
+}
+
+mlbm_status compact_set_band_shape(mlbm_lattice* lat, int rows, int planes) {
+  if (!compact_band_supported(lat, rows))
+    return set_error(MLBM_ERR_ARG,
+                     "one-pass step: the bands' psi planes do not fit shared "
+                     "memory (fewer rows per band, or the two-pass step)");
+  lat->compact.band_rows = rows;
+  lat->compact.band_planes = planes;
+  return MLBM_OK;
+}
+
+template <typename T>
+mlbm_status launch_compact_band(mlbm_lattice* lat, const StepArgs& a,
+                                bool write_u, bool write_rho) {
+  CompactState& c = lat->compact;
+  if (lat->phase != 1)
+    return set_error(MLBM_ERR_STATE, "one-pass step needs the AA phase-1 state");
+  if (!c.cpop_alt) {
+    const cudaError_t e =
+        cudaMalloc(&c.cpop_alt, (size_t)c.cs * Q * pop_elem_bytes(lat->storage));
+    if (e != cudaSuccess) {
+      c.cpop_alt = nullptr;
+      cudaGetLastError();
+      return cuda_fail(e, "one-pass step buffer");
+    }
+  }
+  const BandShape s = band_shape(lat->g, c.band_rows, c.band_planes);
+  const size_t smem = band_smem_bytes(s.hmax, lat->g.lx);
+  if (smem > kBandSmemMax)
+    return set_error(MLBM_ERR_ARG, "one-pass step: band does not fit shared memory");
+  if (mlbm_status st = band_smem_attr<T>(lat->device, smem)) return st;
+  const bool inj = inject_now(lat, a);
+  const T* A = static_cast<const T*>(c.cpop);
+  T* B = static_cast<T*>(c.cpop_alt);
+  const dim3 grid((unsigned)s.nb * (unsigned)s.nc);
+  float* rho = static_cast<float*>(lat->rho);
+  const uint32_t cs = (uint32_t)c.cs;
+  if (write_u)
+    k_band<T, true, true><<<grid, kBandThreads, smem, lat->stream>>>(
+        A, B, cs, c.cinfo, c.wtab, rho, lat->vel, lat->g, lat->phys, a, inj, s);
+  else if (write_rho)
+    k_band<T, true, false><<<grid, kBandThreads, smem, lat->stream>>>(
+        A, B, cs, c.cinfo, c.wtab, rho, lat->vel, lat->g, lat->phys, a, inj, s);
+  else
+    k_band<T, false, false><<<grid, kBandThreads, smem, lat->stream>>>(
+        A, B, cs, c.cinfo, c.wtab, rho, lat->vel, lat->g, lat->phys, a, inj, s);
+  const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(e, "one-pass step launch");
+  std::swap(c.cpop, c.cpop_alt);
+  return MLBM_OK;
+}
+
+template mlbm_status launch_compact_band<float>(mlbm_lattice*, const StepArgs&, bool, bool);
+template mlbm_status launch_compact_band<__half>(mlbm_lattice*, const StepArgs&, bool, bool);
 
 }  // namespace mlbm
