@@ -1,26 +1,36 @@
 """Benchmark of the D3Q19 Shan-Chen time step on B200.
 
-Workload (one GPU): the 200^3 drainage case -- seeded sphere packing
-(radius U[5,15], centres uniform, overlap allowed, added until porosity
-<= 0.50), pores start at rho = 2.0, inlet slab x < 8 held at rho = 0.10,
-outlet plane x = 199 held at rho = 1.95, periodic in y and z, G = -6.0,
-tau = 1.0, G_ads = -1.0 (rhos = -ln(1 - G_ads/G) = 0.182322).  Synthetic
-input: the packing comes from libmlbm's seeded generator.
+Workload (one GPU): the 200^3 drainage case -- the sphere packing of
+``multiphase_lbm_b200/workloads/drainage_200_seed2024.positions`` (radius
+U[5,15], centres uniform, overlap allowed, added until porosity <= 0.50,
+written by that folder's ``make_positions.py``), pores start at rho = 2.0,
+inlet slab x < 8 held at rho = 0.10, outlet plane x = 199 held at rho = 1.95,
+periodic in y and z, G = -6.0, tau = 1.0, G_ads = -1.0
+(rhos = -ln(1 - G_ads/G) = 0.182322).  Both arms read the same positions
+file: this library through mlbm_read_positions, the reference arm through
+the reference's own read_positions.
 
 One bench step = one lattice time step over the whole domain.  ``value`` is
 MLUPS (lattice nodes x steps / s, the reference's convention, all nodes)
-timed on the device with CUDA events around K steps whose inputs are
-resident in HBM (the lattice, 0.6 GB, is far larger than L2, so no flush is
-needed).  ``e2e`` is the same metric through the C ABI with host buffers:
-geometry and initial density copied in from pinned host memory, then every
-step an ``mlbm_iterate`` call and a device->host read of its phase
-statistics, and the final density field copied out.
+timed on the device with CUDA events around blocks of K steps whose inputs
+are resident in HBM (the lattice, >= 0.3 GB, is larger than L2, so no flush
+is needed); blocks are repeated until at least a second has been timed and
+the median block is reported.  FP32 storage is the headline; the FP16-store
+form is timed in the same run (``fp16``).  ``e2e`` is the same metric
+through the C ABI with host buffers: geometry and initial density copied in
+from pinned host memory, then every step an ``mlbm_iterate`` call and a
+device->host read of its phase statistics, and the final density field
+copied out.
 
-``--impl reference`` times the reference's own kernels compiled for the CPU
-(``oracle/_ref``, OpenMP over all host cores) on a bounded sample of the same
-workload.  ``--gpus N`` (under torchrun) runs N independent replicas, one per
-GPU (the single-domain step has no exchange to shard); value = all ranks'
-node updates / the slowest rank's time.
+``--impl reference`` runs the reference's own code: its time step compiled
+for the CPU (``oracle/_ref``, OpenMP over all host cores) on a bounded
+sample of the same workload (the line's ``value``), and its CUDA build
+(``oracle/_ref/ref_cuda_timer_200x200x200``: the reference's unmodified
+kernels between CUDA events, periodic boundaries as the reference has no
+drainage boundary) on the same GPU (``reference_cuda``).  It loads nothing
+of this library.  ``--gpus N`` (under torchrun) runs N independent replicas,
+one per GPU (the single-domain step has no exchange to shard); value = all
+ranks' node updates / the slowest rank's time.
 """
 from __future__ import annotations
 
@@ -30,6 +40,7 @@ import os
 import statistics
 import subprocess
 import sys
+import tempfile
 import threading
 import time
 
@@ -40,6 +51,9 @@ sys.path.insert(0, ROOT)
 
 SHAPE = (200, 200, 200)
 RHO_S = 0.182322  # -ln(1 - G_ads/G) for G_ads = -1, G = -6
+POSITIONS = os.path.join(ROOT, "multiphase_lbm_b200", "workloads",
+                         "drainage_200_seed2024.positions")
+MIN_TIMED_S = 1.0  # timed blocks repeat until this much device time
 
 
 def phys(n=200):
@@ -54,10 +68,59 @@ BYTES_PER_FLUID = {"f32": 152, "f16": 76, "f64": 304}
 
 
 def workload(shape=SHAPE, seed=2024):
+    """(fluid mask, initial density, sphere count) of the n^3 case through
+    this library: the committed positions file at 200^3, the seeded
+    generator at other (profiling) sizes."""
     from multiphase_lbm_b200 import host
-    fluid, spheres = host.generate_packing(shape, 5.0, 15.0, 0.50, seed)
+    if tuple(shape) == SHAPE:
+        fluid, _, n = host.read_positions(POSITIONS, shape)
+    else:
+        fluid, spheres = host.generate_packing(shape, 5.0, 15.0, 0.50, seed)
+        n = len(spheres)
     rho = np.full(shape, 2.0, np.float32)
-    return fluid, rho, len(spheres)
+    return fluid, rho, n
+
+
+def command_file(folder: str) -> str:
+    """The 200^3 case as a command file in the reference's format (read by
+    its read_data, src/multiphase_lbm.cu:619-745): density 2.0 everywhere,
+    the committed positions file, statistics never due, one OpenMP thread
+    per host core this process may use."""
+    text = f"""! 200^3 drainage benchmark packing
+result_folder {folder}/RES
+num_threads {len(os.sched_getaffinity(0))}
+statPeriod 1000000000
+lx 200
+ly 200
+lz 200
+rho0 2.0
+IniPerturbRate 0.0
+G -6.0
+rhos {RHO_S}
+tau 1.0
+rhol_spinodal 0.2726
+rhog_spinodal 0.0484
+resize
+resolution 1
+read_positions {POSITIONS}
+step_max 1000000000
+"""
+    path = os.path.join(folder, "bench_200.txt")
+    with open(path, "w") as fh:
+        fh.write(text)
+    return path
+
+
+def bench_config(fluid_nodes: int, spheres: int, n: int = 200) -> dict:
+    """The workload description both arms print (identical dicts)."""
+    return {"workload": f"drainage {n}^3: spheres r~U[5,15] to porosity 0.50 "
+                        f"(positions file, seed 2024), pores rho 2.0, inlet "
+                        f"x<{phys(n)['inlet_width']} rho 0.10, outlet "
+                        f"x={n - 1} rho 1.95, G -6, tau 1, rhos 0.182322",
+            "lattice": [n, n, n], "fluid_nodes": int(fluid_nodes),
+            "porosity": round(fluid_nodes / n ** 3, 5), "spheres": int(spheres),
+            "l2": "inputs larger than L2 (FP32 populations 0.61 GB, FP16 "
+                  "0.30 GB per step), no flush"}
 
 
 def load_peaks():
@@ -81,7 +144,8 @@ def load_traffic(kernel, storage):
 
 
 # roofline label and launches per step of each step kernel
-KERNEL_INFO = {5: ("wave", "k_cwave (wavefront step, compact layout)", 1),
+KERNEL_INFO = {6: ("band", "k_band (one-pass step, compact layout, two buffers)", 1),
+               5: ("wave", "k_cwave (wavefront step, compact layout)", 1),
                4: ("single-pass", "k_compact_step (single pass, compact layout)", 1),
                3: ("compact", "time step (k_cdensity + k_cupdate, compact layout)", 2),
                2: ("two-pass", "time step (k_density + k_update_zm)", 2),
@@ -106,7 +170,7 @@ class ClockSampler:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.index),
                  f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                 "-lms", "200"], stdout=subprocess.PIPE,
+                 "-lms", "100"], stdout=subprocess.PIPE,
                 stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
@@ -147,83 +211,190 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def cpu_reference_sample(fluid, rho, budget_s=15.0, max_steps=200):
-    """Reference kernels on the host cores (oracle/_ref) at the bench size."""
+# ---- the reference's own code -------------------------------------------------
+
+def reference_read(folder: str):
+    """Geometry and initial density through the reference's own command-file
+    parser and read_positions (oracle/_ref), and its harness at 200^3."""
     import oracle
-    if tuple(fluid.shape) not in oracle.reference_sizes():
+    if SHAPE not in oracle.reference_sizes():
         return None
-    ref = oracle.Reference(fluid.shape)
-    p = oracle.make_params(**PHYS)
-    ref.setup(rho, fluid, p)
+    ref = oracle.Reference(SHAPE)
+    rho, fluid, _, info = ref.driver_read(command_file(folder))
+    ref.setup(rho, fluid, oracle.make_params(**PHYS))
+    return ref, fluid, int(info["solid_count"])
+
+
+def reference_cpu_steps(ref, step0: int, steps: int, budget_s: float):
+    """Time up to `steps` reference steps on the host cores, stopping once
+    `budget_s` is spent: (steps run, seconds)."""
     t0 = time.perf_counter()
+    done = 0
+    while done < steps:
+        ref.step(step0 + done, 1)
+        done += 1
+        if time.perf_counter() - t0 >= budget_s:
+            break
+    return done, time.perf_counter() - t0
+
+
+def cpu_reference_sample(budget_s=15.0, max_steps=200):
+    """cpu_baseline of this library's line: the reference's time step on the
+    host cores, a bounded sample of the 200^3 case."""
+    with tempfile.TemporaryDirectory() as folder:
+        got = reference_read(folder)
+    if got is None:
+        return None
+    ref, fluid, _ = got
     ref.step(0, 1)
-    t1 = time.perf_counter() - t0
-    n = int(max(1, min(max_steps, budget_s / max(t1, 1e-6))))
-    t0 = time.perf_counter()
-    ref.step(1, n)
-    dt = time.perf_counter() - t0
+    n, dt = reference_cpu_steps(ref, 1, max_steps, budget_s)
     cores = len(os.sched_getaffinity(0))
-    mlups = fluid.size * n / dt / 1e6
-    return {"value": round(mlups, 3), "unit": "MLUPS", "cores": cores,
-            "kind": "reference",
-            "sample": f"{n} steps of the 200^3 drainage case (reference "
+    return {"value": round(fluid.size * n / dt / 1e6, 3), "unit": "MLUPS",
+            "cores": cores, "kind": "reference",
+            "sample": f"{n} steps of the 200^3 drainage case (the reference's "
                       f"kernels compiled for the CPU, OpenMP {cores} threads, "
                       f"race-free two-sweep collision)"}
+
+
+def reference_cuda(folder: str, steps: int, warmup: int, device: int):
+    """The reference's CUDA build on this GPU: its unmodified
+    multiphaselbm_iteration timed between CUDA events by
+    oracle/_ref/ref_cuda_timer_200x200x200, blocks of `steps` steps repeated
+    for about a second; median block."""
+    exe = os.path.join(ROOT, "oracle", "_ref", "ref_cuda_timer_200x200x200")
+    if not os.path.exists(exe):
+        return {"unavailable": "oracle/_ref/ref_cuda_timer_200x200x200 not built"}
+    cmd = command_file(folder)
+    # ~3 ms per step: enough blocks for about a second of timed steps
+    repeats = max(3, int(MIN_TIMED_S / (0.003 * steps)) + 1)
+    with ClockSampler(device) as clocks:
+        r = subprocess.run(
+            ["bash", "-c", f"ulimit -s unlimited; exec {exe} {cmd} "
+                           f"{warmup} {steps} {repeats}"],
+            cwd=folder, capture_output=True, text=True, timeout=600)
+    blocks = [float(ln.split()[-1]) for ln in r.stdout.splitlines()
+              if ln.startswith("block ")]
+    if r.returncode != 0 or not blocks:
+        return {"unavailable": f"reference CUDA timer exited {r.returncode}: "
+                               f"{(r.stderr or r.stdout)[-200:]}"}
+    ms = statistics.median(blocks)
+    return {"ms_per_step": round(ms, 4),
+            "value": round(SHAPE[0] * SHAPE[1] * SHAPE[2] / (ms / 1e3) / 1e6, 2),
+            "unit": "MLUPS", "steps": steps, "blocks": len(blocks),
+            "boundaries": "periodic (the reference has no drainage boundary)",
+            "clocks": clocks.summary()}
 
 
 def run_reference_arm(args, rank, world):
     if rank != 0:
         return 0
-    fluid, rho, _ = workload()
-    import oracle
-    if tuple(fluid.shape) not in oracle.reference_sizes():
-        print(json.dumps({"impl": "reference",
-                          "unavailable": "oracle/_ref has no 200^3 build"}))
-        return 0
-    ref = oracle.Reference(fluid.shape)
-    ref.setup(rho, fluid, oracle.make_params(**PHYS))
-    cores = len(os.sched_getaffinity(0))
-    steps_per = 1  # each bench step = a bounded sample of 1 lattice step
-    for w in range(args.warmup):
-        ref.step(w * steps_per, steps_per)
-    t0 = time.perf_counter()
-    for k in range(args.steps):
-        ref.step((args.warmup + k) * steps_per, steps_per)
-    dt = time.perf_counter() - t0
-    mlups = fluid.size * steps_per * args.steps / dt / 1e6
+    with tempfile.TemporaryDirectory() as folder:
+        got = reference_read(folder)
+        if got is None:
+            print(json.dumps({"impl": "reference",
+                              "unavailable": "oracle/_ref has no 200^3 build"}))
+            return 0
+        ref, fluid, spheres = got
+        cores = len(os.sched_getaffinity(0))
+        for w in range(args.warmup):
+            ref.step(w, 1)
+        # each bench step is one lattice step; the sample stops after ~60 s
+        n, dt = reference_cpu_steps(ref, args.warmup, args.steps, 60.0)
+        mlups = fluid.size * n / dt / 1e6
+        cuda = None
+        if not args.no_reference_cuda:
+            cuda = reference_cuda(folder, max(args.steps, 20), args.warmup,
+                                  int(os.environ.get("LOCAL_RANK", "0")))
+    sample = (f"{n} of {args.steps} timed lattice steps (each bench step one "
+              f"lattice step; stops after 60 s) of the 200^3 drainage case")
     line = {
         "impl": "reference", "metric": "MLUPS", "value": round(mlups, 3),
         "unit": "MLUPS", "n_gpus": args.gpus, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": round(dt / args.steps * 1e3, 3),
+        "warmup": args.warmup, "ms_per_step": round(dt / n * 1e3, 3),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f32", "data": "synthetic",
-        "config": {"workload": "drainage 200^3, sphere packing porosity 0.50, "
-                               "inlet x<8 rho 0.10, outlet x=199 rho 1.95",
-                   "sample_steps_per_bench_step": steps_per},
+        "dtype": "f32", "data": "synthetic (seeded sphere packing)",
+        "config": bench_config(int(fluid.sum()), spheres),
         "cpu_baseline": {"value": round(mlups, 3), "unit": "MLUPS",
                          "cores": cores, "kind": "reference",
-                         "sample": f"{steps_per} lattice steps per bench step"},
+                         "sample": sample + f", OpenMP {cores} threads"},
         "e2e": {"value": round(mlups, 3), "unit": "MLUPS",
                 "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
+    if cuda is not None:
+        line["reference_cuda"] = cuda
     print(json.dumps(line))
     return 0
+
+
+# ---- this library ------------------------------------------------------------
+
+def timed_blocks(lat, torch, step, steps, dist):
+    """Blocks of `steps` steps between CUDA events on the lattice's stream
+    (the current stream), repeated until MIN_TIMED_S of device time; returns
+    (median ms per block, blocks, next step)."""
+    from multiphase_lbm_b200.shard import max_over_ranks
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    times = []
+    total = 0.0
+    while total < MIN_TIMED_S * 1e3 or len(times) < 3:
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        ev0.record()
+        lat.iterate(step, steps)
+        ev1.record()
+        torch.cuda.synchronize()
+        step += steps
+        ms = max_over_ranks(ev0.elapsed_time(ev1))
+        times.append(ms)
+        total += ms
+    return statistics.median(times), len(times), step
+
+
+def measure(capi, torch, fluid, rho, storage_name, args, local, dist,
+            kernel_id):
+    """Median device time per step of one storage format."""
+    storage = {"f32": capi.STORE_F32, "f16": capi.STORE_F16,
+               "f64": capi.STORE_F64}[storage_name]
+    params = capi.default_params(**phys(args.size), rho_shift=1.0)
+    lat = capi.Lattice(fluid.shape, storage=storage, device=local)
+    lat.set_params(params)
+    lat.upload(fluid, rho)
+    lat.initialize()
+    if kernel_id is not None:
+        lat.set_step_kernel(kernel_id)
+    if args.band_shape:
+        lat.set_band_shape(*[int(v) for v in args.band_shape.split(",")])
+    if args.wave_shape:
+        lat.set_wave_shape(*[int(v) for v in args.wave_shape.split(",")])
+    kernel = lat.step_kernel
+    lat.iterate(0, args.warmup)
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clocks:
+        ms, blocks, _ = timed_blocks(lat, torch, args.warmup, args.steps, dist)
+    lat.close()
+    return ms / args.steps, blocks, clocks.summary(), kernel
 
 
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--steps", type=int, default=500)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--storage", default="f32", choices=["f32", "f16", "f64"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-fp16", action="store_true")
+    ap.add_argument("--no-reference-cuda", action="store_true")
     ap.add_argument("--size", type=int, default=200,
                     help="lattice edge (profiling runs use a smaller case)")
     ap.add_argument("--kernel", default="auto",
-                    choices=["auto", "wave", "compact", "single-pass", "fused",
-                             "two-pass"])
+                    choices=["auto", "band", "wave", "compact", "single-pass",
+                             "fused", "two-pass"])
+    ap.add_argument("--band-shape", default=None,
+                    help="rows,planes of the one-pass step's bands")
     ap.add_argument("--wave-shape", default=None,
                     help="tile_nodes,lookahead of the wavefront step")
     args = ap.parse_args()
@@ -244,50 +415,20 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
 
     from multiphase_lbm_b200 import capi
-    storage = {"f32": capi.STORE_F32, "f16": capi.STORE_F16,
-               "f64": capi.STORE_F64}[args.storage]
     fluid, rho, nspheres = workload((args.size,) * 3)
     n_nodes = fluid.size
     n_fluid = int(fluid.sum())
-    params = capi.default_params(**phys(args.size), rho_shift=1.0)
-
-    lat = capi.Lattice(fluid.shape, storage=storage, device=local)
-    lat.set_params(params)
-    lat.upload(fluid, rho)
-    lat.initialize()
-    kernel_id = {"auto": capi.KERNEL_AUTO, "wave": capi.KERNEL_WAVE,
-                 "compact": capi.KERNEL_COMPACT,
+    kernel_id = {"auto": None, "band": capi.KERNEL_BAND,
+                 "wave": capi.KERNEL_WAVE, "compact": capi.KERNEL_COMPACT,
                  "single-pass": capi.KERNEL_SINGLE_PASS,
                  "fused": capi.KERNEL_FUSED,
                  "two-pass": capi.KERNEL_TWO_PASS}[args.kernel]
-    lat.set_step_kernel(kernel_id)
-    if args.wave_shape:
-        lat.set_wave_shape(*[int(v) for v in args.wave_shape.split(",")])
-    kname, klabel, klaunches = KERNEL_INFO[lat.step_kernel]
-    step = 0
-    lat.iterate(step, args.warmup)
-    step += args.warmup
-    torch.cuda.synchronize()
 
     # ---- device-timed region (inputs resident) --------------------------
-    ev0 = torch.cuda.Event(enable_timing=True)
-    ev1 = torch.cuda.Event(enable_timing=True)
-    if dist:
-        dist.barrier()
-    torch.cuda.synchronize()
-    with ClockSampler(local) as clocks:
-        ev0.record()
-        lat.iterate(step, args.steps)
-        ev1.record()
-        torch.cuda.synchronize()
-    step += args.steps
-    if dist:
-        dist.barrier()
-    ms = ev0.elapsed_time(ev1)
-    from multiphase_lbm_b200.shard import max_over_ranks
-    t_max = max_over_ranks(ms)
-    s_per_step = t_max / 1e3 / args.steps
-    mlups = n_nodes * world * args.steps / (t_max / 1e3) / 1e6
+    s_per_step, blocks, clocks, kernel = measure(
+        capi, torch, fluid, rho, args.storage, args, local, dist, kernel_id)
+    kname, klabel, klaunches = KERNEL_INFO[kernel]
+    mlups = n_nodes * world / s_per_step / 1e6
 
     # ---- roofline of the time step ----------------------------------------
     peak, peak_kind = load_peaks()
@@ -295,15 +436,34 @@ def main():
     achieved = alg_bytes / s_per_step / 1e9
     traffic = load_traffic(kname, args.storage) if args.size == 200 else None
 
+    fp16 = None
+    if args.storage == "f32" and not args.no_fp16:
+        s16, b16, c16, _ = measure(capi, torch, fluid, rho, "f16", args, local,
+                                   dist, kernel_id)
+        alg16 = n_fluid * BYTES_PER_FLUID["f16"] + n_nodes / 8
+        fp16 = {"ms_per_step": round(s16 * 1e3, 4),
+                "value": round(n_nodes * world / s16 / 1e6, 2), "unit": "MLUPS",
+                "speedup_vs_fp32": round(s_per_step / s16, 3),
+                "roofline": {"achieved": round(alg16 / s16 / 1e9, 1),
+                             "peak": peak, "unit": "GB/s",
+                             "frac": round(alg16 / s16 / 1e9 / peak, 4),
+                             "alg_bytes_per_step": int(alg16),
+                             "traffic": load_traffic(kname, "f16")
+                             if args.size == 200 else None},
+                "timed_blocks": b16, "clocks": c16}
+
     # ---- end to end through the C ABI with host buffers --------------------
     e2e = None
     if not args.no_e2e:
-        e2e = run_e2e(capi, torch, fluid, rho, params, storage, local,
-                      args.steps, dist, kernel_id)
+        e2e = run_e2e(capi, torch, fluid, rho, capi.default_params(
+            **phys(args.size), rho_shift=1.0),
+            {"f32": capi.STORE_F32, "f16": capi.STORE_F16,
+             "f64": capi.STORE_F64}[args.storage],
+            local, args.steps, dist, kernel_id)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline and args.size == 200:
-        cpu = cpu_reference_sample(fluid, rho)
+        cpu = cpu_reference_sample()
 
     line = {
         "metric": "MLUPS", "value": round(mlups, 2), "unit": "MLUPS",
@@ -311,39 +471,36 @@ def main():
         "ms_per_step": round(s_per_step * 1e3, 4), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": args.storage,
         "data": "synthetic (seeded sphere packing)",
-        "config": {"workload": "drainage 200^3: spheres r~U[5,15] to porosity "
-                               "0.50, pores rho 2.0, inlet x<8 rho 0.10, outlet "
-                               "x=199 rho 1.95, G -6, tau 1, rhos 0.182322",
-                   "lattice": list(fluid.shape), "fluid_nodes": n_fluid,
-                   "porosity": round(n_fluid / n_nodes, 5),
-                   "spheres": nspheres, "storage": args.storage,
-                   "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
-                   "l2": "inputs larger than L2 (lattice "
-                         f"{capi.lattice_bytes(fluid.shape, storage) / 1e9:.2f} GB)"},
-        "mflups": round(n_fluid * world * args.steps / (t_max / 1e3) / 1e6, 2),
+        "config": bench_config(n_fluid, nspheres, args.size),
+        "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
+        "timed_blocks": blocks,
+        "mflups": round(n_fluid * world / s_per_step / 1e6, 2),
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1),
                      "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 4),
-                     "traffic": traffic, "peak_kind": peak_kind,
-                     "kernel": klabel,
+                     "traffic": traffic,
+                     "traffic_source": "committed ncu summary "
+                                       "(profiles/traffic.json), not this run",
+                     "peak_kind": peak_kind, "kernel": klabel,
                      "alg_bytes_per_step": int(alg_bytes)},
-        "clocks": clocks.summary(),
-        "gpu_launches": klaunches * args.steps,
+        "clocks": clocks,
+        "gpu_launches": klaunches * args.steps * blocks,
     }
+    if fp16:
+        line["fp16"] = fp16
     if e2e:
         line["e2e"] = e2e
     if cpu:
         line["cpu_baseline"] = cpu
     if rank == 0:
         print(json.dumps(line))
-    lat.close()
     if dist:
         dist.destroy_process_group()
     return 0
 
 
 def run_e2e(capi, torch, fluid, rho, params, storage, device, steps, dist,
-            kernel_id=0):
+            kernel_id=None):
     """MLUPS through the public C ABI with host buffers (pinned).  Every
     step's phase statistics are read back: enqueued without waiting
     (mlbm_phase_stats_async) and read on the host one step later, while the
@@ -355,7 +512,8 @@ def run_e2e(capi, torch, fluid, rho, params, storage, device, steps, dist,
            for _ in range(2)]
     done = [torch.cuda.Event() for _ in range(2)]
     lat = capi.Lattice(fluid.shape, storage=storage, device=device)
-    lat.set_step_kernel(kernel_id)
+    if kernel_id is not None:
+        lat.set_step_kernel(kernel_id)
     lat.set_params(params)
     if dist:
         dist.barrier()
@@ -385,6 +543,7 @@ def run_e2e(capi, torch, fluid, rho, params, storage, device, steps, dist,
     stats_bytes = 8 * capi.STATS_RAW_LEN
     assert len(sat) == steps
     return {"value": round(n * world * steps / dt / 1e6, 2), "unit": "MLUPS",
+            "steps": steps,
             "h2d_bytes_per_step": int((n + 4 * n) / steps),
             "d2h_bytes_per_step": int(stats_bytes + 4 * n / steps)}
 

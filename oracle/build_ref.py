@@ -16,8 +16,9 @@ and compiles with g++:
   oracle/ref_shim.h and oracle/ref_harness.cpp (OpenMP over x);
 * ``oracle/_ref/multiphaselbm_cpu_<lx>x<ly>x<lz>`` -- the reference program
   (src/main.cc) linked against the same objects;
-* ``oracle/_ref/multiphaselbm_cuda_200x200x200`` -- the reference program
-  with its own CUDA kernels, built for sm_100a (timing only).
+* ``oracle/_ref/ref_cuda_timer_200x200x200`` -- the reference's own CUDA
+  time step, built for sm_100a and timed between CUDA events by
+  oracle/ref_cuda_timer.cu (a reported baseline only).
 
 Run: ``python oracle/build_ref.py [--sizes 16x12x10,64x64x64]``.  Without the
 reference sources present (as on a machine that only receives the built
@@ -162,35 +163,41 @@ def build_dropin(sizes=None, force: bool = False) -> list[str]:
     return out
 
 
-# The reference program as the reference builds it for the GPU (its own
-# kernels, src/iteration_host.cu), compiled for sm_100a: only to time the
-# reference's CUDA path on the B200 beside this library.  Not a parity
-# oracle (its collision kernel reads neighbours another thread may be
-# writing, so its results are not deterministic).
+# The reference's own CUDA time step (src/iteration_host.cu, unmodified)
+# with its host driver (src/multiphase_lbm.cu) for the set-up, driven by
+# oracle/ref_cuda_timer.cu, which times multiphaselbm_iteration between CUDA
+# events: the reference's CUDA path measured on the B200 beside this library.
+# Not a parity oracle (its collision kernel reads neighbours another thread
+# may be writing, so its results are not deterministic).
 CUDA_SIZES = ["200x200x200"]
 
 
+def cuda_timer_path(size: str = "200x200x200") -> str:
+    return os.path.join(OUT, f"ref_cuda_timer_{size}")
+
+
 def build_cuda(sizes=None, force: bool = False) -> list[str]:
-    """Build oracle/_ref/multiphaselbm_cuda_<size>."""
+    """Build oracle/_ref/ref_cuda_timer_<size>."""
     if not os.path.isdir(os.path.join(REFERENCE, "include")):
         return []
     nvcc = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
     scratch = os.path.join(tempfile.gettempdir(), "mlbm_ref_build")
     os.makedirs(OUT, exist_ok=True)
+    timer = os.path.join(HERE, "ref_cuda_timer.cu")
     out = []
     for size in sizes or CUDA_SIZES:
-        exe = os.path.join(OUT, f"multiphaselbm_cuda_{size}")
-        if not force and os.path.exists(exe):
+        exe = cuda_timer_path(size)
+        if (not force and os.path.exists(exe)
+                and os.path.getmtime(exe) > os.path.getmtime(timer)):
             out.append(exe)
             continue
         root = _prepare_tree(size, scratch)
-        cmd = [nvcc, "-O3", "-std=c++14", "-w",
+        cmd = [nvcc, "-O3", "-std=c++14", "-w", "-Xcompiler", "-fopenmp",
                "-gencode", "arch=compute_100a,code=sm_100a",
                "-I", os.path.join(root, "include"),
                "-I", os.path.join(root, "external"),
-               os.path.join(root, "src", "iteration_host.cu"),
-               os.path.join(root, "src", "multiphase_lbm.cu"),
-               os.path.join(root, "src", "main.cc"), "-o", exe]
+               timer, os.path.join(root, "src", "iteration_host.cu"),
+               os.path.join(root, "src", "multiphase_lbm.cu"), "-o", exe]
         subprocess.run(cmd, check=True)
         out.append(exe)
     return out

@@ -1,0 +1,137 @@
+"""Parity at the benchmarked configurations, against the oracle.
+
+* The 200^3 drainage case exactly as ``bench.py`` runs it (the committed
+  positions file, pores at rho 2.0, inlet x < 8 at 0.10, outlet x = 199 at
+  1.95, G -6, tau 1, rhos 0.182322): the default step kernel, the one-pass
+  step, the compact two-pass step and the dense two-pass step against the
+  FP32 oracle (oracle/mlbm_oracle.c, bit-exact with the reference's own
+  kernels on this workload: test_bench_workload.py) at steps 1, 2, 10 and
+  100, both AA phases.  FP32 bar: density within 1e-5 relative pointwise,
+  populations and velocity within 1e-5 relative to their largest value.
+  (The configured case goes unstable near step 175 in the reference's own
+  scheme, so the comparison stops at 100.)
+* The same case with FP16 storage (populations stored as half(f - t_i),
+  shift rho0 = 1) against the FP64 oracle over 100 steps: density within
+  FP16_RHO_TOL relative pointwise, saturation within FP16_SAT_TOL.
+* The small periodic case as configured: 64^3, spheres r ~ U[2.5, 7.5] to
+  porosity 0.50, density 0.70 +- 0.01 from the reference's srand(1)/rand()
+  stream, 1,000 steps of phase separation.  Pointwise FP32 bar at steps 1,
+  10 and 100; at step 1,000 (after the unstable growth of phase separation
+  has amplified last-bit differences of exp), the total mass within 1e-6
+  relative and the liquid fraction within 2e-3.
+"""
+import os
+import sys
+
+import numpy as np
+import pytest
+
+import oracle
+from conftest import pointwise_rel_err, rel_err
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+import bench  # noqa: E402
+
+pytestmark = pytest.mark.gpu
+
+FP16_RHO_TOL = 2e-2
+FP16_SAT_TOL = 1e-3
+
+
+def _lattice(capi, fluid, rho, kernel, storage=0, **kw):
+    lat = capi.Lattice(fluid.shape, storage=storage)
+    lat.set_step_kernel(kernel)
+    lat.set_params(capi.default_params(**kw))
+    lat.upload(fluid, rho)
+    lat.initialize()
+    return lat
+
+
+def test_bench_workload_fp32_kernels_match_oracle_100_steps():
+    from multiphase_lbm_b200 import capi
+    fluid, rho, _ = bench.workload()
+    kernels = {"auto": capi.KERNEL_AUTO, "band": capi.KERNEL_BAND,
+               "compact": capi.KERNEL_COMPACT, "two-pass": capi.KERNEL_TWO_PASS}
+    lats = {k: _lattice(capi, fluid, rho, v, **bench.PHYS)
+            for k, v in kernels.items()}
+    port = oracle.Port(rho, fluid, oracle.make_params(**bench.PHYS))
+    m = fluid.astype(bool)
+    step = 0
+    for n in (1, 1, 8, 90):
+        port.step(step, n)
+        r_o, f_o, u_o = port.get("rho"), port.get("f"), port.get("velocity")
+        for name, lat in lats.items():
+            if n > 1:
+                lat.iterate(step, n - 1)
+            lat.iterate(step + n - 1, 1, write_velocity=True)
+            lat.synchronize()
+            e = pointwise_rel_err(lat.field("rho"), r_o, m)
+            assert e <= 1e-5, f"{name} step {step + n}: rho {e:.3e}"
+            e = rel_err(lat.field("f"), f_o, m)
+            assert e <= 1e-5, f"{name} step {step + n}: populations {e:.3e}"
+            e = rel_err(lat.field("velocity")[m], u_o[m])
+            assert e <= 1e-5, f"{name} step {step + n}: velocity {e:.3e}"
+        step += n
+    for lat in lats.values():
+        lat.close()
+
+
+def _saturation(rho, m, rhol=0.2726):
+    return float((rho[m] > rhol).sum()) / float(m.sum())
+
+
+@pytest.mark.parametrize("kernel", ["band", "compact"])
+def test_bench_workload_fp16_against_fp64_oracle(kernel):
+    from multiphase_lbm_b200 import capi
+    fluid, rho, _ = bench.workload()
+    k = capi.KERNEL_BAND if kernel == "band" else capi.KERNEL_COMPACT
+    lat = _lattice(capi, fluid, rho, k, storage=capi.STORE_F16, rho_shift=1.0,
+                   **bench.PHYS)
+    port = oracle.Port(rho, fluid, oracle.make_params(**bench.PHYS), f64=True)
+    m = fluid.astype(bool)
+    lat.iterate(0, 100)
+    port.step(0, 100)
+    r16, r64 = lat.field("rho"), port.get("rho")
+    e = pointwise_rel_err(r16, r64, m)
+    ds = abs(_saturation(r16, m) - _saturation(r64, m))
+    print(f"fp16 {kernel}: rho pointwise {e:.3e}, saturation {ds:.3e}")
+    assert e <= FP16_RHO_TOL, e
+    assert ds <= FP16_SAT_TOL, ds
+    lat.close()
+
+
+def test_small_periodic_case_as_configured_1000_steps():
+    from multiphase_lbm_b200 import capi, host
+    shape = (64, 64, 64)
+    fluid, _ = host.generate_packing(shape, 2.5, 7.5, 0.50, seed=64)
+    rho = host.init_density(shape, 0.70, 0.02 / 0.70)
+    assert abs(float(rho.min()) - 0.69) < 1e-3 and abs(float(rho.max()) - 0.71) < 1e-3
+    kw = dict(G=-6.0, tau=1.0, rhos=0.182322)
+    lat = _lattice(capi, fluid, rho, capi.KERNEL_AUTO, **kw)
+    band = _lattice(capi, fluid, rho, capi.KERNEL_BAND, **kw)
+    port = oracle.Port(rho, fluid, oracle.make_params(**kw))
+    m = fluid.astype(bool)
+    step = 0
+    for n in (1, 9, 90, 900):
+        lat.iterate(step, n)
+        band.iterate(step, n)
+        port.step(step, n)
+        step += n
+        r_g, r_b, r_o = lat.field("rho"), band.field("rho"), port.get("rho")
+        assert np.array_equal(r_g, r_b)  # one-pass == default, bit for bit
+        if step <= 100:
+            e = pointwise_rel_err(r_g, r_o, m)
+            assert e <= 1e-5, f"step {step}: rho {e:.3e}"
+            e = rel_err(lat.field("f"), port.get("f"), m)
+            assert e <= 1e-5, f"step {step}: populations {e:.3e}"
+    s = lat.stats()
+    o = port.phase_stats()
+    dm = abs(s["mass"] - o[7]) / o[7]
+    sat_g, sat_o = _saturation(r_g, m), _saturation(r_o, m)
+    print(f"64^3 step 1000: mass {dm:.3e}, saturation {sat_g:.4f} vs {sat_o:.4f}")
+    assert dm <= 1e-6, dm
+    assert abs(sat_g - sat_o) <= 2e-3
+    # phase separation happened
+    assert 0.05 < sat_o < 0.95
