@@ -286,9 +286,10 @@ mlbm_status mlbm_plane_profile(mlbm_lattice* lat, int64_t* n_fluid_x,
 
 /* Phase statistics without any allocation.  No counterpart in the
  * reference: it exists for callers that cannot call cudaMalloc when they need
- * statistics (inside a CUDA graph capture sequence, under a device-memory
- * budget owned by their own allocator, or embedded in an application that
- * forbids library allocations).  Same results as mlbm_phase_stats, computed
+ * statistics (an application that reserves the GPU's memory up front for its
+ * own pool, or a host that forbids libraries to allocate because cudaMalloc
+ * may synchronise the device and take unbounded time).  Same results as
+ * mlbm_phase_stats, computed
  * from fields the caller owns: rho_dev (float) and is_fluid_dev (uint8,
  * nonzero = fluid), both device arrays in the reference layout [x][y][z]
  * (z fastest); the EOS and thresholds come from *params.  Runs on `stream`
@@ -297,8 +298,9 @@ mlbm_status mlbm_plane_profile(mlbm_lattice* lat, int64_t* n_fluid_x,
  * loads the library, kept until exit), so nx may not exceed
  * MLBM_NOALLOC_MAX_LX (MLBM_ERR_ARG otherwise).  The first call on each
  * device looks up the array's device address; make it before any stream
- * capture starts.  Calls share the array: calls that overlap on the GPU race
- * and must be serialised by the caller. */
+ * capture starts, and make no call on a device after cudaDeviceReset (the
+ * kept address belongs to the reset context).  Calls share the array: calls
+ * that overlap on the GPU race and must be serialised by the caller. */
 #define MLBM_NOALLOC_MAX_LX 4096
 mlbm_status mlbm_phase_stats_noalloc(const float* rho_dev,
                                      const uint8_t* is_fluid_dev, int32_t nx,

@@ -1,13 +1,16 @@
 // noalloc.cu -- mlbm_phase_stats_noalloc: the phase statistics of
 // mlbm_phase_stats computed without allocating any memory.
 //
-// Who needs it: callers that must not (or cannot) call cudaMalloc at the
-// moment they want statistics -- code running between the capture calls of
-// a CUDA graph, hosts that run under a fixed device-memory budget handed out
-// by their own allocator, or plugins embedded in an application that owns
-// the device and forbids allocations from libraries.  They pass device
-// pointers to fields they already own; this entry point adds no allocation
-// of its own (no cudaMalloc, cudaFree or allocating library routine).
+// Who needs it: callers that cannot call cudaMalloc when they want
+// statistics -- an application that reserves the GPU's memory up front for
+// its own pool (a library's cudaMalloc would then fail, or take memory the
+// pool has promised elsewhere), and solver loops embedded in a host that
+// forbids libraries to allocate because cudaMalloc and cudaFree may
+// synchronise the device and take unbounded time.  They pass device pointers
+// to fields they already own; this entry point adds no allocation of its own
+// (no cudaMalloc, cudaFree or allocating library routine).  It does copy the
+// result row to a host array and waits for the caller's stream before it
+// returns.
 //
 // Its scratch -- one row of partial sums per x-plane plus one result row --
 // lives in a file-scope __device__ array of fixed size.  Every GPU that loads
@@ -22,7 +25,9 @@
 // In host code the array's name is only a host-side stand-in, not a device
 // address.  The first call on each device therefore looks the real address
 // up with cudaGetSymbolAddress (with that device current) and keeps it; make
-// that first call on a device before any stream capture begins.
+// that first call on a device before any stream capture begins.  The kept
+// address belongs to the device's primary context: a process that resets
+// the device (cudaDeviceReset) must not call this entry point afterwards.
 #include <cuda_runtime.h>
 
 #include <cstring>
