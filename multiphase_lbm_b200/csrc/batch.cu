@@ -314,6 +314,7 @@ mlbm_status mlbm_batch_create(int32_t storage, int32_t device,
   int ndev = 0;
   BCUDA(cudaGetDeviceCount(&ndev), "cudaGetDeviceCount");
   if (device < 0 || device >= ndev) return bfail(MLBM_ERR_CUDA, "device not available");
+  mlbm::DeviceGuard restore_device;
   BCUDA(cudaSetDevice(device), "cudaSetDevice");
   mlbm_batch* b = new (std::nothrow) mlbm_batch();
   if (!b) return bfail(MLBM_ERR_NOMEM, "host allocation");
@@ -331,6 +332,7 @@ mlbm_status mlbm_batch_create(int32_t storage, int32_t device,
 
 mlbm_status mlbm_batch_destroy(mlbm_batch* b) {
   if (!b) return MLBM_OK;
+  mlbm::DeviceGuard restore_device;
   cudaSetDevice(b->device);
   if (b->stream) cudaStreamSynchronize(b->stream);
   drop_graph(b);
@@ -352,6 +354,7 @@ mlbm_status mlbm_batch_add(mlbm_batch* b, int32_t nx, int32_t ny, int32_t nz,
                            const float* rho, int64_t step0, int32_t* id) {
   if (!b || !params || !is_fluid || !rho || !id)
     return bfail(MLBM_ERR_ARG, "null argument");
+  mlbm::DeviceGuard restore_device;
   BCUDA(cudaSetDevice(b->device), "cudaSetDevice");
   mlbm_lattice* lat = nullptr;
   if (mlbm_status st = mlbm_lattice_create(nx, ny, nz, b->storage, b->device, &lat))
@@ -418,6 +421,7 @@ mlbm_status mlbm_batch_iterate(mlbm_batch* b, int32_t nsteps, int32_t reverse,
   if (!b) return bfail(MLBM_ERR_ARG, "null batch");
   if (nsteps < 0) return bfail(MLBM_ERR_ARG, "negative step count");
   if (nsteps == 0) return MLBM_OK;
+  mlbm::DeviceGuard restore_device;
   BCUDA(cudaSetDevice(b->device), "cudaSetDevice");
   if (b->dirty)
     if (mlbm_status st = rebuild(b)) return st;

@@ -433,6 +433,7 @@ mlbm_status mlbm_lattice_create(int32_t lx, int32_t ly, int32_t lz,
   if (device < 0 || device >= ndev)
     return fail(MLBM_ERR_CUDA, "device %d not available (%d devices)", device,
                 ndev);
+  mlbm::DeviceGuard restore_device;
   CUDA_TRY(cudaSetDevice(device), "cudaSetDevice");
   mlbm_lattice* lat = new (std::nothrow) mlbm_lattice();
   if (!lat) return fail(MLBM_ERR_NOMEM, "host allocation failed");
@@ -478,6 +479,7 @@ mlbm_status mlbm_lattice_create(int32_t lx, int32_t ly, int32_t lz,
 
 mlbm_status mlbm_lattice_destroy(mlbm_lattice* lat) {
   if (!lat) return MLBM_OK;
+  mlbm::DeviceGuard restore_device;
   cudaSetDevice(lat->device);
   if (lat->stream_owned_sync) cudaStreamSynchronize(lat->stream);
   cudaFree(lat->pop);
@@ -555,24 +557,28 @@ static mlbm_status upload_rho_impl(mlbm_lattice* lat, const float* src,
 mlbm_status mlbm_upload_fluid_mask(mlbm_lattice* lat, const uint8_t* f) {
   if (mlbm_status st = check_lat(lat)) return st;
   if (!f) return fail(MLBM_ERR_ARG, "null mask");
+  DeviceGuard restore_device;
   if (mlbm_status st = activate(lat)) return st;
   return upload_mask_impl(lat, f, cudaMemcpyDefault);
 }
 mlbm_status mlbm_upload_fluid_mask_device(mlbm_lattice* lat, const uint8_t* f) {
   if (mlbm_status st = check_lat(lat)) return st;
   if (!f) return fail(MLBM_ERR_ARG, "null mask");
+  DeviceGuard restore_device;
   if (mlbm_status st = activate(lat)) return st;
   return upload_mask_impl(lat, f, cudaMemcpyDeviceToDevice);
 }
 mlbm_status mlbm_upload_rho(mlbm_lattice* lat, const float* r) {
   if (mlbm_status st = check_lat(lat)) return st;
   if (!r) return fail(MLBM_ERR_ARG, "null rho");
+  DeviceGuard restore_device;
   if (mlbm_status st = activate(lat)) return st;
   return upload_rho_impl(lat, r, cudaMemcpyDefault);
 }
 mlbm_status mlbm_upload_rho_device(mlbm_lattice* lat, const float* r) {
   if (mlbm_status st = check_lat(lat)) return st;
   if (!r) return fail(MLBM_ERR_ARG, "null rho");
+  DeviceGuard restore_device;
   if (mlbm_status st = activate(lat)) return st;
   return upload_rho_impl(lat, r, cudaMemcpyDeviceToDevice);
 }
@@ -582,6 +588,7 @@ mlbm_status mlbm_initialize(mlbm_lattice* lat) {
   if (!lat->has_params || !lat->has_mask || !lat->has_rho)
     return fail(MLBM_ERR_STATE,
                 "initialize needs params, fluid mask and rho first");
+  DeviceGuard restore_device;
   if (mlbm_status st = activate(lat)) return st;
   mlbm_status st;
   switch (lat->storage) {
@@ -609,6 +616,7 @@ mlbm_status mlbm_iterate(mlbm_lattice* lat, int64_t step0, int32_t nsteps,
                 "iterate on a slab lattice: step it with mlbm_step_pass and "
                 "exchange its halos between the passes");
   if (nsteps == 0) return MLBM_OK;
+  DeviceGuard restore_device;
   if (mlbm_status st = activate(lat)) return st;
   switch (lat->storage) {
     case MLBM_STORE_F32:
@@ -624,6 +632,7 @@ mlbm_status mlbm_download_field_device(mlbm_lattice* lat, int32_t field,
                                        int32_t dtype, void* dev_out) {
   if (mlbm_status st = check_lat(lat)) return st;
   if (!dev_out) return fail(MLBM_ERR_ARG, "null output");
+  DeviceGuard restore_device;
   if (mlbm_status st = activate(lat)) return st;
   if (field == MLBM_FIELD_FLUID) {
     if (dtype != MLBM_DTYPE_U8)
@@ -649,6 +658,7 @@ mlbm_status mlbm_download_field(mlbm_lattice* lat, int32_t field,
   const Geom& g = lat->g;
   const size_t esz = dtype == MLBM_DTYPE_F64 ? 8 : (dtype == MLBM_DTYPE_U8 ? 1 : 4);
   const size_t bytes = (size_t)g.lx * g.ly * g.lz * field_components(field) * esz;
+  DeviceGuard restore_device;
   if (mlbm_status st = activate(lat)) return st;
   if (mlbm_status st = ensure_staging(lat, bytes)) return st;
   if (mlbm_status st = mlbm_download_field_device(lat, field, dtype, lat->staging))
@@ -675,6 +685,7 @@ mlbm_status stats_enqueue(mlbm_lattice* lat, double* h) {
     return fail(MLBM_ERR_STATE,
                 "phase statistics of a slab would count its halo planes: "
                 "gather the slabs' own planes first");
+  DeviceGuard restore_device;
   if (mlbm_status st = activate(lat)) return st;
   // a lattice held in the fluid-only layout is walked through its node
   // table (no lanes idle on solid nodes); otherwise the dense grid
@@ -782,6 +793,7 @@ mlbm_status mlbm_plane_profile(mlbm_lattice* lat, int64_t* n_fluid_x,
   if (mlbm_status st = check_lat(lat)) return st;
   if (!n_fluid_x || !n_liquid_x) return fail(MLBM_ERR_ARG, "null output");
   if (!lat->initialized) return fail(MLBM_ERR_STATE, "profile before initialize");
+  DeviceGuard restore_device;
   if (mlbm_status st = activate(lat)) return st;
   const int lx = lat->g.lx;
   const size_t bytes = 2 * (size_t)lx * sizeof(unsigned long long);
@@ -835,6 +847,7 @@ mlbm_status mlbm_set_tuning(mlbm_lattice* lat, int32_t rows_per_item,
   if (rows_per_item < 0 || plane_lag < 0 || rows_per_item > 16 ||
       (rows_per_item & (rows_per_item - 1)) != 0 || plane_lag > 64)
     return fail(MLBM_ERR_ARG, "invalid tuning (rows 0 or 1..16 power of two, lag 0..64)");
+  DeviceGuard restore_device;
   if (mlbm_status st = activate(lat)) return st;
   // the progress counters count this tiling's planes: restart them
   CUDA_TRY(cudaStreamSynchronize(lat->stream), "tuning sync");
@@ -850,6 +863,7 @@ mlbm_status mlbm_set_update_shape(mlbm_lattice* lat, int32_t rows,
   if (mlbm_status st = check_lat(lat)) return st;
   if (rows < 1 || rows > 8 || planes < 1 || planes > 1024)
     return fail(MLBM_ERR_ARG, "invalid update shape %d x %d", rows, planes);
+  DeviceGuard restore_device;
   if (mlbm_status st = activate(lat)) return st;
   CUDA_TRY(cudaStreamSynchronize(lat->stream), "update shape");
   return setup_update(lat, rows, planes);
@@ -874,6 +888,7 @@ mlbm_status mlbm_set_wave_shape(mlbm_lattice* lat, int32_t tile_nodes,
   if (tile_nodes < 32 || tile_nodes > 65536 || lookahead < 0 || lookahead > 256)
     return fail(MLBM_ERR_ARG, "invalid wavefront shape %d nodes, %d planes ahead",
                 tile_nodes, lookahead);
+  DeviceGuard restore_device;
   if (mlbm_status st = activate(lat)) return st;
   CUDA_TRY(cudaStreamSynchronize(lat->stream), "wavefront shape");
   return compact_set_wave_shape(lat, tile_nodes, lookahead);
@@ -884,6 +899,7 @@ mlbm_status mlbm_set_compact_shape(mlbm_lattice* lat, int32_t rows,
   if (mlbm_status st = check_lat(lat)) return st;
   if (rows < 2 || rows > 64 || planes < 2 || planes > 4096)
     return fail(MLBM_ERR_ARG, "invalid compact shape %d x %d", rows, planes);
+  DeviceGuard restore_device;
   if (mlbm_status st = activate(lat)) return st;
   CUDA_TRY(cudaStreamSynchronize(lat->stream), "compact shape");
   return compact_set_shape(lat, rows, planes);
@@ -895,6 +911,7 @@ mlbm_status mlbm_autotune(mlbm_lattice* lat, int64_t step0,
   if (mlbm_status st = check_lat(lat)) return st;
   if (!lat->initialized) return fail(MLBM_ERR_STATE, "autotune before initialize");
   if (trial_steps < 1) trial_steps = 2;
+  DeviceGuard restore_device;
   if (mlbm_status st = activate(lat)) return st;
   if (effective_kernel(lat) == MLBM_KERNEL_COMPACT) {
     // one thread per fluid node: nothing to tune
@@ -966,6 +983,7 @@ mlbm_status mlbm_autotune(mlbm_lattice* lat, int64_t step0,
 
 mlbm_status mlbm_synchronize(mlbm_lattice* lat) {
   if (mlbm_status st = check_lat(lat)) return st;
+  DeviceGuard restore_device;
   if (mlbm_status st = activate(lat)) return st;
   CUDA_TRY(cudaStreamSynchronize(lat->stream), "synchronize");
   return check_device_error(lat);

@@ -329,6 +329,7 @@ extern "C" mlbm_status mlbm_cluster_stats_gpu(
   const long long n = (long long)lx * ly * lz;
   if (n >= (1LL << 31))
     return set_error(MLBM_ERR_ARG, "cluster_stats_gpu: more than 2^31 nodes");
+  mlbm::DeviceGuard restore_device;
   CL_TRY(cudaSetDevice(device), "cluster_stats_gpu");
   const Dims d{lx, ly, lz, n};
   const unsigned grid = (unsigned)((n + 255) / 256);

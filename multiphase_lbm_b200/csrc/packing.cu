@@ -136,6 +136,7 @@ extern "C" mlbm_status mlbm_generate_packing_gpu(
   const long long n = (long long)lx * ly * lz;
   if (max_spheres >= (int64_t)UINT_MAX)
     return set_error(MLBM_ERR_ARG, "generate_packing_gpu: too many spheres");
+  mlbm::DeviceGuard restore_device;
   cudaError_t e = cudaSetDevice(device);
   if (e != cudaSuccess) return cuda_fail(e, "generate_packing_gpu");
   Buffers b;

@@ -200,6 +200,7 @@ bool ring_jobs(const mlbm_slab_ring* r, int what, std::vector<HaloJob>& out,
 extern "C" {
 
 mlbm_status mlbm_set_slab(mlbm_lattice* lat, int32_t enable) {
+  DeviceGuard restore_device;
   if (mlbm_status st = ready_for_passes(lat, "set_slab")) return st;
   if (enable && lat->g.lz < 3)
     return set_error(MLBM_ERR_ARG,
@@ -212,6 +213,7 @@ mlbm_status mlbm_set_slab(mlbm_lattice* lat, int32_t enable) {
 mlbm_status mlbm_step_pass(mlbm_lattice* lat, int64_t step, int32_t pass,
                            int32_t reverse, uint32_t inject_type,
                            uint32_t flags) {
+  DeviceGuard restore_device;
   if (pass != 0 && pass != 1)
     return set_error(MLBM_ERR_ARG, "step_pass: pass must be 0 (density) or 1 (update)");
   if (mlbm_status st = ready_for_passes(lat, "step_pass")) return st;
@@ -240,6 +242,7 @@ mlbm_status mlbm_step_pass(mlbm_lattice* lat, int64_t step, int32_t pass,
 
 mlbm_status mlbm_halo_segments(mlbm_lattice* lat, int32_t kind, int32_t side,
                                void** ptrs, int64_t* bytes, int32_t* count) {
+  DeviceGuard restore_device;
   if (!ptrs || !bytes || !count)
     return set_error(MLBM_ERR_ARG, "halo_segments: null output");
   if (side != 0 && side != 1)
@@ -257,6 +260,7 @@ mlbm_status mlbm_halo_segments(mlbm_lattice* lat, int32_t kind, int32_t side,
 
 mlbm_status mlbm_slab_ring_create(mlbm_lattice* const* slabs, int32_t n,
                                   mlbm_slab_ring** out) {
+  DeviceGuard restore_device;
   if (!slabs || n < 1 || !out)
     return set_error(MLBM_ERR_ARG, "slab_ring_create: bad arguments");
   *out = nullptr;
@@ -322,6 +326,7 @@ mlbm_status mlbm_slab_ring_create(mlbm_lattice* const* slabs, int32_t n,
 }
 
 mlbm_status mlbm_slab_ring_exchange(mlbm_slab_ring* r, int32_t what) {
+  DeviceGuard restore_device;
   if (!r) return set_error(MLBM_ERR_ARG, "slab_ring_exchange: null ring");
   if (what < 0 || what >= kRingKinds)
     return set_error(MLBM_ERR_ARG, "slab_ring_exchange: unknown exchange");
@@ -365,6 +370,7 @@ mlbm_status mlbm_slab_ring_exchange(mlbm_slab_ring* r, int32_t what) {
 }
 
 mlbm_status mlbm_slab_ring_destroy(mlbm_slab_ring* r) {
+  DeviceGuard restore_device;
   if (!r) return MLBM_OK;
   cudaSetDevice(r->device);
   ring_free(r);
