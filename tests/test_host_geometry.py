@@ -75,7 +75,8 @@ def test_voxeliser_against_reference_live(tmp_path, shape, res):
 def test_example_positions_file_porosity():
     """The reference's example packing at 200^3, resolution 1: porosity
     0.50187 (the reference voxelisation)."""
-    path = "/root/reference/example_positions_file"
+    from oracle import build_ref
+    path = os.path.join(build_ref.REFERENCE, "example_positions_file")
     if not os.path.exists(path):
         pytest.skip("reference example file not present")
     fluid, _, count = host.read_positions(path, (200, 200, 200), 1.0)
