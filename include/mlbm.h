@@ -284,6 +284,35 @@ mlbm_status mlbm_stats_from_raw(mlbm_lattice* lat, const double* raw,
 mlbm_status mlbm_plane_profile(mlbm_lattice* lat, int64_t* n_fluid_x,
                                int64_t* n_liquid_x);
 
+/* ---- Exact checkpoints --------------------------------------------------------
+ * The whole state of a lattice in its stored precision: populations (FP32,
+ * FP16 bits or FP64, every node, dense layout), AA phase, density field,
+ * fluid mask and parameters, plus the caller's step counter, with a
+ * versioned header and a hash of the payload.  Loading an image into a
+ * lattice of the same size and storage and stepping on gives, bit for bit,
+ * what the saved lattice gives.  Replaces the reference's read_densities
+ * resume (src/multiphase_lbm.cu:112-132), which reloads a "%.4e" density
+ * field and restarts the populations from equilibrium.
+ *   mlbm_checkpoint_bytes  size of the image of `lat` (header included);
+ *   mlbm_checkpoint_save   write the image to host memory `image` (pinned or
+ *                          pageable, at least that many bytes); synchronises
+ *                          the lattice's stream;
+ *   mlbm_checkpoint_load   restore params, mask, density and populations
+ *                          from an image (MLBM_ERR_ARG: not an image, other
+ *                          size or storage, truncated, hash mismatch);
+ *                          *step (optional) receives the saved counter;
+ *   mlbm_checkpoint_write / _read   the same through a file.
+ * Slab lattices are refused (MLBM_ERR_STATE). */
+mlbm_status mlbm_checkpoint_bytes(const mlbm_lattice* lat, uint64_t* bytes);
+mlbm_status mlbm_checkpoint_save(mlbm_lattice* lat, int64_t step, void* image,
+                                 uint64_t bytes);
+mlbm_status mlbm_checkpoint_load(mlbm_lattice* lat, const void* image,
+                                 uint64_t bytes, int64_t* step);
+mlbm_status mlbm_checkpoint_write(mlbm_lattice* lat, int64_t step,
+                                  const char* path);
+mlbm_status mlbm_checkpoint_read(mlbm_lattice* lat, const char* path,
+                                 int64_t* step);
+
 /* Phase statistics without any allocation.  No counterpart in the
  * reference: it exists for callers that cannot call cudaMalloc when they need
  * statistics (an application that reserves the GPU's memory up front for its

@@ -37,7 +37,7 @@ CXXFLAGS = ["-O2", "-std=c++17", "-fPIC", "-fopenmp", "-ffp-contract=off",
 
 CUDA_SOURCES = ["capi.cu", "compat.cu", "persistent.cu", "noalloc.cu",
                 "batch.cu", "compact.cu", "packing.cu", "clusters_gpu.cu",
-                "slab.cu"]
+                "slab.cu", "checkpoint.cu"]
 HOST_SOURCES = ["host/driver.cpp", "host/geometry.cpp", "host/output.cpp",
                 "host/clusters.cpp"]
 CLI_SOURCE = "host/main.cpp"

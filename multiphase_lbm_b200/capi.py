@@ -131,6 +131,12 @@ SIGNATURES = [
     ("mlbm_slab_ring_create", C.c_int, [_VP, C.c_int32, C.POINTER(_VP)]),
     ("mlbm_slab_ring_exchange", C.c_int, [_VP, C.c_int32]),
     ("mlbm_slab_ring_destroy", C.c_int, [_VP]),
+    ("mlbm_checkpoint_bytes", C.c_int, [_VP, C.POINTER(C.c_uint64)]),
+    ("mlbm_checkpoint_save", C.c_int, [_VP, C.c_int64, _VP, C.c_uint64]),
+    ("mlbm_checkpoint_load", C.c_int, [_VP, _VP, C.c_uint64,
+                                       C.POINTER(C.c_int64)]),
+    ("mlbm_checkpoint_write", C.c_int, [_VP, C.c_int64, C.c_char_p]),
+    ("mlbm_checkpoint_read", C.c_int, [_VP, C.c_char_p, C.POINTER(C.c_int64)]),
     ("mlbm_phase_stats_noalloc", C.c_int, [_VP, _VP, C.c_int32, C.c_int32,
                                            C.c_int32, C.POINTER(Params), _VP,
                                            C.POINTER(Stats)]),
@@ -222,6 +228,35 @@ class Lattice:
         """Work items of the wavefront step: fluid nodes per item and the
         lead of the density tiles over the update tiles, in planes."""
         check(lib().mlbm_set_wave_shape(self.h, tile_nodes, lookahead))
+
+    def checkpoint(self, step: int, out: "np.ndarray | None" = None) -> np.ndarray:
+        """Exact image of the lattice's state (uint8 array; `out`, if given,
+        must be a large enough uint8 array, e.g. pinned memory)."""
+        n = C.c_uint64()
+        check(lib().mlbm_checkpoint_bytes(self.h, C.byref(n)))
+        if out is None:
+            out = np.empty(n.value, np.uint8)
+        if out.dtype != np.uint8 or out.nbytes < n.value:
+            raise ValueError(f"checkpoint needs a uint8 buffer of {n.value} bytes")
+        check(lib().mlbm_checkpoint_save(self.h, int(step), out.ctypes.data,
+                                         out.nbytes))
+        return out
+
+    def restore(self, image: np.ndarray) -> int:
+        """Load an image made by checkpoint(); returns its step counter."""
+        a = np.ascontiguousarray(image, np.uint8)
+        step = C.c_int64()
+        check(lib().mlbm_checkpoint_load(self.h, a.ctypes.data, a.nbytes,
+                                         C.byref(step)))
+        return int(step.value)
+
+    def write_checkpoint(self, path: str, step: int) -> None:
+        check(lib().mlbm_checkpoint_write(self.h, int(step), path.encode()))
+
+    def read_checkpoint(self, path: str) -> int:
+        step = C.c_int64()
+        check(lib().mlbm_checkpoint_read(self.h, path.encode(), C.byref(step)))
+        return int(step.value)
 
     def set_band_shape(self, rows: int = 4, planes: int = 24) -> None:
         """Tiling of KERNEL_BAND: rows per band (y) and planes per chunk (z)."""

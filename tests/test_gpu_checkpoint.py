@@ -1,0 +1,100 @@
+"""Exact checkpoints (mlbm_checkpoint_*): save a lattice at step k, load the
+image into a fresh lattice of the same size and storage, run m more steps:
+density, populations and velocity are bit-identical to the lattice that ran
+k + m steps uninterrupted -- FP32, FP16 and FP64 storage, from either AA
+phase (odd and even k), through memory and through a file, with the step
+kernels that hold the state in the fluid-only layout.  Images of another
+size or storage, truncated or corrupted images are refused."""
+import numpy as np
+import pytest
+
+from conftest import sphere_case
+
+pytestmark = pytest.mark.gpu
+
+DRAIN = dict(G=-5.0, rhos=0.223144, tau=1.0, inlet_width=3, outlet_width=1,
+             rho_inlet=0.17, rho_outlet=1.90, rho_shift=1.0)
+SHAPE = (48, 40, 36)
+
+
+def _lattice(capi, fluid, rho, storage, kernel):
+    lat = capi.Lattice(fluid.shape, storage=storage)
+    lat.set_step_kernel(kernel)
+    lat.set_params(capi.default_params(**DRAIN))
+    lat.upload(fluid, rho)
+    lat.initialize()
+    return lat
+
+
+def _state(lat, step):
+    lat.iterate(step, 1, write_velocity=True)
+    return lat.field("rho"), lat.field("f"), lat.field("velocity")
+
+
+@pytest.mark.parametrize("storage,kernel", [(0, 0), (0, 6), (1, 0), (1, 6),
+                                            (2, 0), (0, 2)])
+@pytest.mark.parametrize("k", [7, 10])
+def test_resume_is_bit_identical(storage, kernel, k):
+    from multiphase_lbm_b200 import capi
+    fluid, rho = sphere_case(SHAPE, seed=3 + k, rmin=2.0, rmax=4.5,
+                             porosity=0.55, rho0=1.9, amp=0.05)
+    a = _lattice(capi, fluid, rho, storage, kernel)
+    a.iterate(0, k)
+    image = a.checkpoint(k)
+    a.iterate(k, 9)
+    want = _state(a, k + 9)
+    b = capi.Lattice(SHAPE, storage=storage)
+    b.set_step_kernel(kernel)
+    assert b.restore(image) == k
+    b.iterate(k, 9)
+    got = _state(b, k + 9)
+    for u, v in zip(got, want):
+        assert np.array_equal(u, v)
+    a.close()
+    b.close()
+
+
+def test_resume_through_a_file(tmp_path):
+    from multiphase_lbm_b200 import capi
+    fluid, rho = sphere_case(SHAPE, seed=1, rmin=2.0, rmax=4.5, porosity=0.55,
+                             rho0=1.9, amp=0.05)
+    a = _lattice(capi, fluid, rho, 1, capi.KERNEL_BAND)
+    a.iterate(0, 5)
+    path = str(tmp_path / "lattice.ckpt")
+    a.write_checkpoint(path, 5)
+    a.iterate(5, 6)
+    want = a.field("f")
+    b = capi.Lattice(SHAPE, storage=1)
+    assert b.read_checkpoint(path) == 5
+    b.iterate(5, 6)
+    assert np.array_equal(b.field("f"), want)
+    a.close()
+    b.close()
+
+
+def test_refuses_foreign_truncated_and_corrupted_images():
+    from multiphase_lbm_b200 import capi
+    fluid, rho = sphere_case(SHAPE, seed=2, rmin=2.0, rmax=4.5, porosity=0.55,
+                             rho0=1.9, amp=0.05)
+    a = _lattice(capi, fluid, rho, 0, 0)
+    a.iterate(0, 3)
+    image = a.checkpoint(3)
+    for lat in (capi.Lattice((48, 40, 35)), capi.Lattice(SHAPE, storage=1)):
+        with pytest.raises(capi.MlbmError):
+            lat.restore(image)
+        lat.close()
+    b = capi.Lattice(SHAPE)
+    with pytest.raises(capi.MlbmError):
+        b.restore(image[: len(image) - 1])
+    bad = image.copy()
+    bad[len(bad) // 2] ^= 1
+    with pytest.raises(capi.MlbmError, match="corrupted"):
+        b.restore(bad)
+    bad = image.copy()
+    bad[0] ^= 1
+    with pytest.raises(capi.MlbmError, match="not a checkpoint"):
+        b.restore(bad)
+    with pytest.raises(capi.MlbmError):
+        capi.Lattice(SHAPE).checkpoint(0)  # not initialised
+    a.close()
+    b.close()
