@@ -145,11 +145,8 @@ def load_traffic(kernel, storage):
 
 # roofline label and launches per step of each step kernel
 KERNEL_INFO = {6: ("band", "k_band (one-pass step, compact layout, two buffers)", 1),
-               5: ("wave", "k_cwave (wavefront step, compact layout)", 1),
-               4: ("single-pass", "k_compact_step (single pass, compact layout)", 1),
                3: ("compact", "time step (k_cdensity + k_cupdate, compact layout)", 2),
-               2: ("two-pass", "time step (k_density + k_update_zm)", 2),
-               1: ("fused", "k_step_fused (persistent)", 1)}
+               2: ("two-pass", "time step (k_density + k_update_zm)", 2)}
 
 
 class ClockSampler:
@@ -366,8 +363,6 @@ def measure(capi, torch, fluid, rho, storage_name, args, local, dist,
         lat.set_step_kernel(kernel_id)
     if args.band_shape:
         lat.set_band_shape(*[int(v) for v in args.band_shape.split(",")])
-    if args.wave_shape:
-        lat.set_wave_shape(*[int(v) for v in args.wave_shape.split(",")])
     kernel = lat.step_kernel
     lat.iterate(0, args.warmup)
     torch.cuda.synchronize()
@@ -391,12 +386,9 @@ def main():
     ap.add_argument("--size", type=int, default=200,
                     help="lattice edge (profiling runs use a smaller case)")
     ap.add_argument("--kernel", default="auto",
-                    choices=["auto", "band", "wave", "compact", "single-pass",
-                             "fused", "two-pass"])
+                    choices=["auto", "band", "compact", "two-pass"])
     ap.add_argument("--band-shape", default=None,
                     help="rows,planes of the one-pass step's bands")
-    ap.add_argument("--wave-shape", default=None,
-                    help="tile_nodes,lookahead of the wavefront step")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -419,9 +411,7 @@ def main():
     n_nodes = fluid.size
     n_fluid = int(fluid.sum())
     kernel_id = {"auto": None, "band": capi.KERNEL_BAND,
-                 "wave": capi.KERNEL_WAVE, "compact": capi.KERNEL_COMPACT,
-                 "single-pass": capi.KERNEL_SINGLE_PASS,
-                 "fused": capi.KERNEL_FUSED,
+                 "compact": capi.KERNEL_COMPACT,
                  "two-pass": capi.KERNEL_TWO_PASS}[args.kernel]
 
     # ---- device-timed region (inputs resident) --------------------------

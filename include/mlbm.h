@@ -175,83 +175,62 @@ mlbm_status mlbm_iterate(mlbm_lattice* lat, int64_t step0, int32_t nsteps,
 /* Which kernels advance the lattice:
  *   TWO_PASS     a density launch and an update launch per step over the
  *                dense layout; bit-identical to the reference's kernels;
- *   FUSED        one cooperative launch per step, the two passes interleaved
- *                plane by plane; bit-identical to TWO_PASS;
  *   COMPACT      the two passes over a fluid-only population layout (solid
  *                nodes own no population storage), one thread per fluid
- *                node; bit-identical to TWO_PASS.  FP32 / FP16 storage, at
- *                most 2048 x 2048 x 1024 nodes;
- *   SINGLE_PASS  one launch per step over the fluid-only layout: the
- *                populations are read and written once per step and psi of
- *                the next step is accumulated from the outputs.  FP32 / FP16
- *                storage, ly, lz >= 4.  The collision is the same; psi is
- *                formed from a differently ordered sum of the same
- *                populations, so results agree with TWO_PASS to rounding (not
- *                bit for bit) and are deterministic;
- *   WAVE         the two passes over the fluid-only layout in ONE persistent
- *                launch per step: density tiles run a few planes ahead of
- *                the update tiles (a wavefront along z), so the update reads
- *                the populations back from L2 and DRAM sees them once per
- *                step.  Bit-identical to TWO_PASS; same limits as COMPACT;
+ *                node pair; bit-identical to TWO_PASS.  FP32 / FP16 storage,
+ *                at most 2048 x 2048 x 1024 nodes;
  *   BAND         ONE launch per step over the fluid-only layout with two
  *                population buffers: the launch reads the step's
  *                populations from one buffer and pushes the new ones into
- *                the other, so no block waits for another; a block forms
- *                psi of a band of rows (plus one halo row on either side) in
- *                shared memory plane by plane and updates the band one plane
- *                behind, so DRAM sees the populations once per step.
- *                Bit-identical to TWO_PASS; FP32 / FP16 storage, whole
- *                lattices (not slabs), same size limits as COMPACT; a
- *                second population buffer is allocated on first use;
+ *                the other, so no block waits for another; in each block,
+ *                density warps form psi of a band of rows (plus one halo
+ *                row on either side) in shared memory plane by plane, and
+ *                update warps follow a few planes behind, so DRAM sees the
+ *                populations about once per step.  Bit-identical to
+ *                TWO_PASS; FP32 / FP16 storage, whole lattices (not slabs),
+ *                same size limits as COMPACT; a second population buffer is
+ *                allocated on first use;
  *   AUTO         (default) COMPACT where supported, else TWO_PASS.
- * The state moves between the layouts on demand (the dense buffers stay
- * allocated; the fluid-only layout adds 19 populations and 14 words per
- * fluid node, allocated on first use). */
+ * (Values 1, 4 and 5 belonged to step kernels this library no longer has;
+ * they are refused.)  The state moves between the layouts on demand (the
+ * dense buffers stay allocated; the fluid-only layout adds 19 populations
+ * and 8 bytes of node table per fluid node, allocated on first use). */
 #define MLBM_KERNEL_AUTO 0
-#define MLBM_KERNEL_FUSED 1
 #define MLBM_KERNEL_TWO_PASS 2
 #define MLBM_KERNEL_COMPACT 3
-#define MLBM_KERNEL_SINGLE_PASS 4
-#define MLBM_KERNEL_WAVE 5
 #define MLBM_KERNEL_BAND 6
 mlbm_status mlbm_set_step_kernel(mlbm_lattice* lat, int32_t kind);
 /* The kernel the next mlbm_iterate runs (AUTO resolved); -1 for NULL. */
 int32_t mlbm_get_step_kernel(const mlbm_lattice* lat);
-/* Work items of the WAVE step: `tile_nodes` fluid nodes per item (32..65536,
- * default 1024) and the lead of the density tiles over the update tiles in
- * planes (0..256, default 4). */
-mlbm_status mlbm_set_wave_shape(mlbm_lattice* lat, int32_t tile_nodes,
-                                int32_t lookahead);
 /* Tiling of the BAND step: bands of about `rows` rows (y, 1..64) and chunks
  * of about `planes` planes (z, 1..1024), one block per band and chunk.
- * Default 4 x 24.  MLBM_ERR_ARG when a band's psi planes do not fit shared
- * memory (4 x (rows + 2) x (lx + 2) floats). */
+ * Default 4 x 24.  MLBM_ERR_ARG when a band's ring of psi planes does not
+ * fit shared memory (6 x (rows + 2) x (lx + 2) floats). */
 mlbm_status mlbm_set_band_shape(mlbm_lattice* lat, int32_t rows,
                                 int32_t planes);
-/* Tiling of the SINGLE_PASS step: a block walks `rows` full x-rows (y) through
- * `planes` planes (z); at least two tiles along y and z, each at least two
- * rows / planes deep.  Default 4 x 8. */
-mlbm_status mlbm_set_compact_shape(mlbm_lattice* lat, int32_t rows,
-                                   int32_t planes);
-/* Tuning of the fused kernel: tile rows (the tile is 32 x rows nodes of an
- * (x, y) plane; 0 = automatic, else 1, 2, 4, 8 or 16) and the lag in planes
- * between a plane's density pass and its update pass (0 = 4, at least 2). */
-mlbm_status mlbm_set_tuning(mlbm_lattice* lat, int32_t rows_per_item,
-                            int32_t plane_lag);
 /* Shape of the two-pass update kernel: tile rows (block = 32 x rows
  * threads, 1..8) and planes walked per block (1..1024).  Default 4 x 16. */
 mlbm_status mlbm_set_update_shape(mlbm_lattice* lat, int32_t rows,
                                   int32_t planes);
 /* Time candidate shapes of the lattice's step kernel (update shape for
- * TWO_PASS, tiling for SINGLE_PASS, tile nodes x lookahead for WAVE; COMPACT
- * has none: out = {0, 0}, no steps) and keep the fastest.  The trial steps are
+ * TWO_PASS, rows x planes for BAND; COMPACT has none: out = {0, 0}, no
+ * steps) and keep the fastest.  The trial steps are
  * real steps (step0, step0+1, ...): the lattice advances by *steps_done of
  * them.  out (optional, 2 ints) receives rows, planes. */
 mlbm_status mlbm_autotune(mlbm_lattice* lat, int64_t step0,
                           int32_t trial_steps, int32_t* out,
                           int32_t* steps_done);
+/* Limit of the step kernels' bounded device waits (hand-overs between the
+ * warps of one block in the BAND step), in nanoseconds; 0 = the default,
+ * one second.  A wait that runs out ends the launch with the device error
+ * flag set: mlbm_synchronize then reports MLBM_ERR_TIMEOUT. */
+mlbm_status mlbm_set_wait_limit(mlbm_lattice* lat, uint64_t ns);
+/* Testing the wait limit: the next BAND step launch makes one block wait on
+ * a barrier that nothing completes, so the limit runs out (MLBM_ERR_STATE
+ * for other step kernels).  The lattice must be initialised again after. */
+mlbm_status mlbm_test_stall_wait(mlbm_lattice* lat);
 /* Wait for the lattice's stream and report a device-side failure (a bounded
- * wait of the fused or wavefront kernel that ran out: MLBM_ERR_TIMEOUT; the
+ * wait of a step kernel that ran out: MLBM_ERR_TIMEOUT; the
  * lattice must then be initialised again). */
 mlbm_status mlbm_synchronize(mlbm_lattice* lat);
 

@@ -35,7 +35,7 @@ CXXFLAGS = ["-O2", "-std=c++17", "-fPIC", "-fopenmp", "-ffp-contract=off",
             "-Wall", "-I", os.path.join(ROOT, "include"), "-I", CSRC,
             "-I", "/usr/local/cuda/include"]
 
-CUDA_SOURCES = ["capi.cu", "compat.cu", "persistent.cu", "noalloc.cu",
+CUDA_SOURCES = ["capi.cu", "compat.cu", "noalloc.cu",
                 "batch.cu", "compact.cu", "packing.cu", "clusters_gpu.cu",
                 "slab.cu", "checkpoint.cu"]
 HOST_SOURCES = ["host/driver.cpp", "host/geometry.cpp", "host/output.cpp",

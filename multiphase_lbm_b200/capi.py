@@ -23,8 +23,7 @@ ITER_WRITE_VELOCITY = 1
 HALO_PSI_EDGE, HALO_PSI_GHOST, HALO_POP_EDGE, HALO_POP_GHOST = 0, 1, 2, 3
 HALO_MAX_SEGMENTS = 5
 STATS_RAW_LEN = 15
-(KERNEL_AUTO, KERNEL_FUSED, KERNEL_TWO_PASS, KERNEL_COMPACT,
- KERNEL_SINGLE_PASS, KERNEL_WAVE, KERNEL_BAND) = 0, 1, 2, 3, 4, 5, 6
+KERNEL_AUTO, KERNEL_TWO_PASS, KERNEL_COMPACT, KERNEL_BAND = 0, 2, 3, 6
 Q = 19
 
 STATUS = {0: "MLBM_OK", 1: "MLBM_ERR_ARG", 2: "MLBM_ERR_CUDA",
@@ -113,12 +112,11 @@ SIGNATURES = [
     ("mlbm_plane_profile", C.c_int, [_VP, _VP, _VP]),
     ("mlbm_lattice_info", C.c_int, [_VP, _VP, _VP, _VP, _VP]),
     ("mlbm_set_step_kernel", C.c_int, [_VP, C.c_int32]),
-    ("mlbm_set_tuning", C.c_int, [_VP, C.c_int32, C.c_int32]),
     ("mlbm_synchronize", C.c_int, [_VP]),
     ("mlbm_set_update_shape", C.c_int, [_VP, C.c_int32, C.c_int32]),
-    ("mlbm_set_compact_shape", C.c_int, [_VP, C.c_int32, C.c_int32]),
-    ("mlbm_set_wave_shape", C.c_int, [_VP, C.c_int32, C.c_int32]),
     ("mlbm_set_band_shape", C.c_int, [_VP, C.c_int32, C.c_int32]),
+    ("mlbm_set_wait_limit", C.c_int, [_VP, C.c_uint64]),
+    ("mlbm_test_stall_wait", C.c_int, [_VP]),
     ("mlbm_get_step_kernel", C.c_int32, [_VP]),
     ("mlbm_autotune", C.c_int, [_VP, C.c_int64, C.c_int32, _VP, _VP]),
     ("mlbm_set_slab", C.c_int, [_VP, C.c_int32]),
@@ -212,9 +210,6 @@ class Lattice:
     def set_step_kernel(self, kind: int) -> None:
         check(lib().mlbm_set_step_kernel(self.h, kind))
 
-    def set_tuning(self, rows_per_item: int = 0, plane_lag: int = 0) -> None:
-        check(lib().mlbm_set_tuning(self.h, rows_per_item, plane_lag))
-
     def set_update_shape(self, rows: int = 4, planes: int = 16) -> None:
         check(lib().mlbm_set_update_shape(self.h, rows, planes))
 
@@ -223,11 +218,6 @@ class Lattice:
         """The kernel the next iterate runs (KERNEL_COMPACT, ... ; AUTO
         resolved)."""
         return int(lib().mlbm_get_step_kernel(self.h))
-
-    def set_wave_shape(self, tile_nodes: int = 1024, lookahead: int = 4) -> None:
-        """Work items of the wavefront step: fluid nodes per item and the
-        lead of the density tiles over the update tiles, in planes."""
-        check(lib().mlbm_set_wave_shape(self.h, tile_nodes, lookahead))
 
     def checkpoint(self, step: int, out: "np.ndarray | None" = None) -> np.ndarray:
         """Exact image of the lattice's state (uint8 array; `out`, if given,
@@ -258,13 +248,17 @@ class Lattice:
         check(lib().mlbm_checkpoint_read(self.h, path.encode(), C.byref(step)))
         return int(step.value)
 
+    def set_wait_limit(self, ns: int) -> None:
+        """Limit of the step kernels' bounded device waits (0 = 1 s)."""
+        check(lib().mlbm_set_wait_limit(self.h, int(ns)))
+
+    def test_stall_wait(self) -> None:
+        """Make one wait of the next BAND launch run out (testing)."""
+        check(lib().mlbm_test_stall_wait(self.h))
+
     def set_band_shape(self, rows: int = 4, planes: int = 24) -> None:
         """Tiling of KERNEL_BAND: rows per band (y) and planes per chunk (z)."""
         check(lib().mlbm_set_band_shape(self.h, rows, planes))
-
-    def set_compact_shape(self, rows: int = 4, planes: int = 8) -> None:
-        """Tiling of the single-pass step (rows along y, planes along z)."""
-        check(lib().mlbm_set_compact_shape(self.h, rows, planes))
 
     def autotune(self, step0: int, trial_steps: int = 4):
         """Pick the shape of the lattice's step kernel by timing; returns

@@ -12,16 +12,28 @@
 // any node's populations at any time, and no block waits for another.
 //
 // Work item = one band of rows [y0, y1) of every plane of a chunk [z0, z1).
-// A block marches the chunk plane by plane.  For plane z + 1 it forms rho
-// and psi of its rows plus one halo row on either side (y0 - 1 and y1,
-// periodic) into a ring of four shared-memory psi planes; after one barrier
-// it updates the own rows of plane z with psi of planes z - 1, z, z + 1 from
-// shared memory.  The halo rows belong to the neighbouring bands, whose
-// blocks read them at about the same time, and the update re-reads the rows
-// the density phase has just loaded: both come from L2, so DRAM sees every
-// population once per step (plus two planes per chunk at the chunk edges).
-// Four ring slots let the density phase of the next plane overwrite the
-// slot the update has finished with, with one barrier per plane.
+// A block marches the chunk plane by plane (even chunks upward, odd ones
+// downward, so a plane shared by two chunks is visited by both at the start
+// or both at the end of their marches and comes from DRAM once).  Its warps
+// are split in two groups:
+//   density warps  form rho and psi of the band's rows plus one halo row on
+//                  either side (periodic) for each plane of the march into a
+//                  ring of kBandSlots shared-memory psi planes;
+//   update warps   update the band's own rows of plane z once psi of planes
+//                  z - 1, z, z + 1 is in the ring: force, collision, push.
+// The groups hand ring slots over through mbarriers (full: the density warps
+// have written the plane; empty: the update warps are done with it), so the
+// density warps run up to kBandSlots - 3 planes ahead: their DRAM reads
+// overlap the update warps' arithmetic instead of alternating with it.  The
+// halo rows belong to the neighbouring bands, whose blocks read them at about
+// the same time, and the update re-reads rows the density warps have just
+// loaded: both come from L2, so DRAM sees every population about once per
+// step.
+//
+// Every wait is bounded in time: a wait that runs out (wait_ns) raises the
+// error flag and its group leaves the kernel; the other group's waits then
+// run out too, so the launch always ends.  `stall` (a test of that path)
+// makes block 0's update warps wait on a barrier nothing arrives at.
 //
 // Per node the arithmetic is the two-pass kernels': rho summed in order
 // i = 0..18 plus injection, psi_of, collide2 of pair.cuh (two nodes per
@@ -35,16 +47,20 @@
 #pragma once
 
 #include "compact2.cuh"
+#include "update_tma.cuh"
 
 namespace mlbm {
 
-constexpr int kBandThreads = 128;
-constexpr int kBandSlots = 4;
+constexpr int kBandD = 128;  // density warps' threads
+constexpr int kBandU = 128;  // update warps' threads
+constexpr int kBandThreads = kBandD + kBandU;
+constexpr int kBandSlots = 6;
 
-// Shared memory of a block: kBandSlots planes of (hmax + 2) rows of
-// (lx + 2) psi values (ghost columns at 0 and lx + 1).
+// Shared memory of a block: 2 * kBandSlots mbarriers, then kBandSlots planes
+// of (hmax + 2) rows of (lx + 2) psi values (ghost columns 0 and lx + 1).
+constexpr size_t kBandBarBytes = 2 * kBandSlots * sizeof(uint64_t) + 16;
 __host__ __device__ inline size_t band_smem_bytes(int hmax, int lx) {
-  return (size_t)kBandSlots * (hmax + 2) * (lx + 2) * sizeof(float);
+  return kBandBarBytes + (size_t)kBandSlots * (hmax + 2) * (lx + 2) * sizeof(float);
 }
 
 // First compact index of row y of plane z (y in [0, ly]; row ly is the next
@@ -95,96 +111,154 @@ __device__ __forceinline__ BandNode band_node(uint2 ci) {
   return n;
 }
 
+__device__ __forceinline__ void band_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar))
+               : "memory");
+}
+__device__ __forceinline__ unsigned long long band_clock_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+// Wait for the phase of `bar` with parity `parity`; false (error flag set)
+// once wait_ns nanoseconds have passed.
+__device__ __forceinline__ bool band_wait(uint64_t* bar, unsigned parity,
+                                          unsigned long long wait_ns,
+                                          int* err) {
+  if (mbar_try_wait(bar, parity)) return true;
+  const unsigned long long t0 = band_clock_ns();
+  while (!mbar_try_wait(bar, parity))
+    if (band_clock_ns() - t0 > wait_ns) {
+      atomicExch(err, 1);
+      return false;
+    }
+  return true;
+}
+
 struct BandShape {
   int nb, nc;  // bands along y, chunks along z
   int hmax;    // rows of the tallest band
 };
 
 template <typename T, bool WRITE_RHO, bool WRITE_U>
-__global__ void __launch_bounds__(kBandThreads, 4)
+__global__ void __launch_bounds__(kBandThreads, 2)
     k_band(const T* __restrict__ A, T* __restrict__ B, uint32_t cs,
            const uint2* __restrict__ cinfo, const uint2* __restrict__ wtab,
-           float* __restrict__ rho_out, float* __restrict__ vel, Geom g,
-           Phys p, StepArgs a, bool inj, BandShape s) {
-  extern __shared__ float sp[];
+           float* __restrict__ rho_out, float* __restrict__ vel,
+           int* __restrict__ err, Geom g, Phys p, StepArgs a, bool inj,
+           BandShape s, unsigned long long wait_ns, bool stall) {
+  extern __shared__ __align__(16) unsigned char band_smem[];
+  uint64_t* full = reinterpret_cast<uint64_t*>(band_smem);
+  uint64_t* empty = full + kBandSlots;
+  uint64_t* never = empty + kBandSlots;  // the stall test's barrier
+  float* sp = reinterpret_cast<float*>(band_smem + kBandBarBytes);
   const int band = blockIdx.x % s.nb, chunk = blockIdx.x / s.nb;
   const int y0 = (int)((long long)band * g.ly / s.nb);
   const int y1 = (int)((long long)(band + 1) * g.ly / s.nb);
   const int z0 = (int)((long long)chunk * g.lz / s.nc);
   const int z1 = (int)((long long)(chunk + 1) * g.lz / s.nc);
+  const int nplanes = z1 - z0;
+  // even chunks march up the planes, odd ones down
+  const int dir = (chunk & 1) ? -1 : 1;
+  const int zfirst = dir > 0 ? z0 : z1 - 1;  // first plane updated
   const int P = g.lx + 2;               // psi row pitch in shared memory
   const int SE = (s.hmax + 2) * P;      // psi plane
   const int rows = y1 - y0;
   const float shift = p.rho_shift;
-  const float psi_solid = psi_of<float>(p, p.rhos);
   // all rows when the band and its halo wrap onto themselves
   const bool all_rows = rows + 2 >= g.ly;
 
-  // rho and psi of the band's rows and halo rows of plane zz (periodic) into
-  // its ring slot
-  auto density = [&](int zz) {
-    const int zw = zz < 0 ? zz + g.lz : (zz >= g.lz ? zz - g.lz : zz);
-    float* slot = sp + ((zz - z0 + 1) & (kBandSlots - 1)) * SE;
-    int ra[2], rb[2], nr = 1;
-    if (all_rows) {
-      ra[0] = 0; rb[0] = g.ly;
-    } else if (y0 == 0) {
-      ra[0] = 0; rb[0] = y1 + 1; ra[1] = g.ly - 1; rb[1] = g.ly; nr = 2;
-    } else if (y1 == g.ly) {
-      ra[0] = y0 - 1; rb[0] = g.ly; ra[1] = 0; rb[1] = 1; nr = 2;
-    } else {
-      ra[0] = y0 - 1; rb[0] = y1 + 1;
+  if (threadIdx.x == 0) {
+    for (int k = 0; k < kBandSlots; ++k) {
+      mbar_init(&full[k], kBandD);
+      mbar_init(&empty[k], kBandU);
     }
-    for (int r = 0; r < nr; ++r) {
-      const int kf = band_row_start(wtab, g, zw, ra[r]);
-      const int ke = band_row_start(wtab, g, zw, rb[r]);
-      for (int t = (kf & ~1) + 2 * (int)threadIdx.x; t < ke;
-           t += 2 * kBandThreads) {
-        const BandNode na = band_node(__ldg(cinfo + t));
-        const BandNode nbn = band_node(__ldg(cinfo + t + 1));
-        const bool va = t >= kf && (na.nb & NB_SELF);
-        const bool vb = t + 1 < ke && (nbn.nb & NB_SELF);
-        if (!va && !vb) continue;
-        float2 f[Q];
-        if ((va && !na.kind) || (vb && !nbn.kind)) {
-          band_gather<T>(A, cs, t, shift, f);
-        } else {
-#pragma unroll
-          for (int i = 0; i < Q; ++i) f[i] = p_dup(0.f);
-        }
-        float2 d = p_dup(0.f);
-#pragma unroll
-        for (int i = 0; i < Q; ++i) d = p_add(d, f[i]);
-        d.x = na.kind ? slab_density(p, na.kind) : inject_on(p, g, a, inj, na.y, d.x);
-        d.y = nbn.kind ? slab_density(p, nbn.kind) : inject_on(p, g, a, inj, nbn.y, d.y);
-        // a row's shared-memory rows: j = y - (y0 - 1) (mod ly), and j + ly
-        // when the band wraps onto itself
-        auto put = [&](const BandNode& n, float v) {
-          int j = n.y - y0 + 1;
-          if (j < 0) j += g.ly;
-          if (j >= g.ly) j -= g.ly;
-          for (; j < rows + 2; j += g.ly) {
-            float* row = slot + j * P;
-            row[n.x + 1] = v;
-            if (n.x == 0) row[g.lx + 1] = v;
-            if (n.x == g.lx - 1) row[0] = v;
-          }
-        };
-        if (va) put(na, psi_of<float>(p, d.x));
-        if (vb) put(nbn, psi_of<float>(p, d.y));
-      }
-    }
-  };
+    mbar_init(never, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
 
-  // force, collision and push of the band's own rows of plane z
-  auto update = [&](int z) {
-    const float* sm = sp + ((z - z0) & (kBandSlots - 1)) * SE;      // z - 1
-    const float* s0 = sp + ((z - z0 + 1) & (kBandSlots - 1)) * SE;  // z
-    const float* spl = sp + ((z - z0 + 2) & (kBandSlots - 1)) * SE; // z + 1
+  if (threadIdx.x < kBandD) {
+    // ---- density warps: planes j = 0 .. nplanes + 1 of the march --------
+    const int td = threadIdx.x;
+    for (int j = 0; j < nplanes + 2; ++j) {
+      const int k = j % kBandSlots;
+      // the slot's previous plane (j - kBandSlots) released by the update
+      if (j >= kBandSlots &&
+          !band_wait(&empty[k], (unsigned)((j / kBandSlots - 1) & 1), wait_ns, err))
+        return;
+      const int zz = zfirst + (j - 1) * dir;
+      const int zw = zz < 0 ? zz + g.lz : (zz >= g.lz ? zz - g.lz : zz);
+      float* slot = sp + k * SE;
+      int ra[2], rb[2], nr = 1;
+      if (all_rows) {
+        ra[0] = 0; rb[0] = g.ly;
+      } else if (y0 == 0) {
+        ra[0] = 0; rb[0] = y1 + 1; ra[1] = g.ly - 1; rb[1] = g.ly; nr = 2;
+      } else if (y1 == g.ly) {
+        ra[0] = y0 - 1; rb[0] = g.ly; ra[1] = 0; rb[1] = 1; nr = 2;
+      } else {
+        ra[0] = y0 - 1; rb[0] = y1 + 1;
+      }
+      for (int r = 0; r < nr; ++r) {
+        const int kf = band_row_start(wtab, g, zw, ra[r]);
+        const int ke = band_row_start(wtab, g, zw, rb[r]);
+        for (int t = (kf & ~1) + 2 * td; t < ke; t += 2 * kBandD) {
+          const BandNode na = band_node(__ldg(cinfo + t));
+          const BandNode nbn = band_node(__ldg(cinfo + t + 1));
+          const bool va = t >= kf && (na.nb & NB_SELF);
+          const bool vb = t + 1 < ke && (nbn.nb & NB_SELF);
+          if (!va && !vb) continue;
+          float2 f[Q];
+          if ((va && !na.kind) || (vb && !nbn.kind)) {
+            band_gather<T>(A, cs, t, shift, f);
+          } else {
+#pragma unroll
+            for (int i = 0; i < Q; ++i) f[i] = p_dup(0.f);
+          }
+          float2 d = p_dup(0.f);
+#pragma unroll
+          for (int i = 0; i < Q; ++i) d = p_add(d, f[i]);
+          d.x = na.kind ? slab_density(p, na.kind) : inject_on(p, g, a, inj, na.y, d.x);
+          d.y = nbn.kind ? slab_density(p, nbn.kind) : inject_on(p, g, a, inj, nbn.y, d.y);
+          // a row's shared-memory rows: j = y - (y0 - 1) (mod ly), and
+          // j + ly when the band wraps onto itself
+          auto put = [&](const BandNode& n, float v) {
+            int jr = n.y - y0 + 1;
+            if (jr < 0) jr += g.ly;
+            if (jr >= g.ly) jr -= g.ly;
+            for (; jr < rows + 2; jr += g.ly) {
+              float* row = slot + jr * P;
+              row[n.x + 1] = v;
+              if (n.x == 0) row[g.lx + 1] = v;
+              if (n.x == g.lx - 1) row[0] = v;
+            }
+          };
+          if (va) put(na, psi_of<float>(p, d.x));
+          if (vb) put(nbn, psi_of<float>(p, d.y));
+        }
+      }
+      band_arrive(&full[k]);
+    }
+    return;
+  }
+
+  // ---- update warps: plane u of the march needs march planes u, u+1, u+2 --
+  const int tu = threadIdx.x - kBandD;
+  const float psi_solid = psi_of<float>(p, p.rhos);
+  if (stall && blockIdx.x == 0 && !band_wait(never, 0u, wait_ns, err)) return;
+  for (int u = 0; u < nplanes; ++u) {
+    for (int j = u == 0 ? 0 : u + 2; j <= u + 2; ++j)
+      if (!band_wait(&full[j % kBandSlots], (unsigned)((j / kBandSlots) & 1),
+                     wait_ns, err))
+        return;
+    const int z = zfirst + u * dir;
+    const float* s0 = sp + ((u + 1) % kBandSlots) * SE;
+    const float* sm = sp + ((dir > 0 ? u : u + 2) % kBandSlots) * SE;   // z - 1
+    const float* spl = sp + ((dir > 0 ? u + 2 : u) % kBandSlots) * SE;  // z + 1
     const int kf = band_row_start(wtab, g, z, y0);
     const int ke = band_row_start(wtab, g, z, y1);
-    for (int t = (kf & ~1) + 2 * (int)threadIdx.x; t < ke;
-         t += 2 * kBandThreads) {
+    for (int t = (kf & ~1) + 2 * tu; t < ke; t += 2 * kBandU) {
       BandNode na = band_node(__ldg(cinfo + t));
       BandNode nbn = band_node(__ldg(cinfo + t + 1));
       const bool va = t >= kf && (na.nb & NB_SELF);
@@ -264,14 +338,7 @@ __global__ void __launch_bounds__(kBandThreads, 4)
       if (va) push(t, na, 0);
       if (vb) push(t + 1, nbn, 1);
     }
-  };
-
-  density(z0 - 1);
-  density(z0);
-  for (int z = z0; z < z1; ++z) {
-    density(z + 1);
-    __syncthreads();
-    update(z);
+    band_arrive(&empty[u % kBandSlots]);
   }
 }
 

@@ -431,7 +431,6 @@ mlbm_status mlbm_batch_iterate(mlbm_batch* b, int32_t nsteps, int32_t reverse,
   for (mlbm_lattice* l : b->dom)
     if (l) {
       l->phase = (l->phase + nsteps) & 1;
-      l->compact.parts_valid = false;  // the single-pass part sums are stale
     }
   return MLBM_OK;
 }

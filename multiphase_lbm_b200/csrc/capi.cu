@@ -18,7 +18,6 @@
 #include "capi_internal.h"
 #include "io_kernels.cuh"
 #include "kernels.cuh"
-#include "persistent.cuh"
 #include "update_tma.cuh"
 
 using namespace mlbm;
@@ -217,15 +216,9 @@ mlbm_status launch_steps(mlbm_lattice* lat, int64_t step0, int32_t nsteps,
                          int32_t reverse, uint32_t inject_type,
                          uint32_t flags) {
   const int kind = effective_kernel(lat);
-  const bool fused = kind == MLBM_KERNEL_FUSED && lat->fused.ok;
-  if (kind == MLBM_KERNEL_FUSED && !lat->fused.ok)
-    return fail(MLBM_ERR_ARG, "fused kernel does not fit this lattice");
-  bool compact = false, single = false, wave = false, band = false;
+  bool compact = false, band = false;
   if constexpr (!std::is_same<T, double>::value) {
-    compact = kind == MLBM_KERNEL_COMPACT || kind == MLBM_KERNEL_SINGLE_PASS ||
-              kind == MLBM_KERNEL_WAVE || kind == MLBM_KERNEL_BAND;
-    single = kind == MLBM_KERNEL_SINGLE_PASS;
-    wave = kind == MLBM_KERNEL_WAVE;
+    compact = kind == MLBM_KERNEL_COMPACT || kind == MLBM_KERNEL_BAND;
     band = kind == MLBM_KERNEL_BAND;
   }
   if ((flags & MLBM_ITER_WRITE_VELOCITY) && !lat->vel) {
@@ -238,10 +231,6 @@ mlbm_status launch_steps(mlbm_lattice* lat, int64_t step0, int32_t nsteps,
              "velocity clear");
   }
   if (compact) {
-    // the single-pass step reads the part sums of the step before it: take
-    // them again from the populations if another kernel ran last
-    if (single && lat->compact.active && !lat->compact.parts_valid)
-      if (mlbm_status st = compact_leave(lat)) return st;
     if (mlbm_status st = compact_enter(lat)) return st;
   } else {
     if (mlbm_status st = compact_leave(lat)) return st;
@@ -256,16 +245,11 @@ mlbm_status launch_steps(mlbm_lattice* lat, int64_t step0, int32_t nsteps,
     // two-pass step gets there
     const bool one_pass = band && lat->phase == 1;
     if constexpr (!std::is_same<T, double>::value) {
-      if (single) st = launch_compact<T>(lat, a, out);
-      else if (wave) st = launch_compact_wave<T>(lat, a, wu, last);
-      else if (one_pass) st = launch_compact_band<T>(lat, a, wu, last);
+      if (one_pass) st = launch_compact_band<T>(lat, a, wu, last);
       else if (compact) st = launch_compact_two_pass<T>(lat, a, wu, last);
-      else if (fused) st = launch_fused<T>(lat, a, out);
       else st = launch_two_pass<T>(lat, a, wu, last);
-      lat->compact.parts_valid = single;
     } else {
-      if (fused) st = launch_fused<T>(lat, a, out);
-      else st = launch_two_pass<T>(lat, a, wu, last);
+      st = launch_two_pass<T>(lat, a, wu, last);
     }
     if (st) return st;
     if (!one_pass) lat->phase ^= 1;
@@ -342,20 +326,17 @@ size_t field_components(int32_t field) {
 }
 
 // After a stream synchronisation: report (and clear) a wait timeout raised by
-// the fused kernel.  The interrupted step left the lattice inconsistent.
+// a step kernel.  The interrupted step left the lattice inconsistent.
 mlbm_status check_device_error(mlbm_lattice* lat) {
   int h = 0;
   CUDA_TRY(cudaMemcpy(&h, lat->err, sizeof(int), cudaMemcpyDeviceToHost),
            "error flag read");
   if (!h) return MLBM_OK;
   cudaMemset(lat->err, 0, sizeof(int));
-  cudaMemset(lat->pdone, 0, sizeof(unsigned) * max_tiles(lat->g));
-  lat->fused_epoch = 0;
-  compact_reset_wave(lat);
   lat->initialized = false;
   return fail(MLBM_ERR_TIMEOUT,
-              "a bounded wait of the time step (fused or wavefront kernel) ran "
-              "out; the lattice must be initialised again");
+              "a bounded wait of the time step ran out; the lattice must be "
+              "initialised again");
 }
 
 mlbm_status ensure_staging(mlbm_lattice* lat, size_t bytes) {
@@ -440,8 +421,6 @@ mlbm_status mlbm_lattice_create(int32_t lx, int32_t ly, int32_t lz,
   lat->device = device;
   lat->storage = storage;
   lat->g = make_geom(lx, ly, lz);
-  lat->fused = fused_shape(lat->g, storage, 0, 0);
-  lat->compact.supported = compact_supported(lx, ly, lz, storage);
   lat->compact.two_pass_ok = compact_two_pass_supported(lx, ly, lz, storage);
   const size_t np = (size_t)lat->g.plane;
   const size_t mask_words = (size_t)lz * ly * lat->g.wpr;
@@ -455,10 +434,7 @@ mlbm_status mlbm_lattice_create(int32_t lx, int32_t ly, int32_t lz,
   alloc((void**)&lat->rho_init, np * sizeof(float));
   alloc((void**)&lat->mask, mask_words * sizeof(uint32_t));
   alloc((void**)&lat->nbw, np * sizeof(uint32_t));
-  const size_t ncount = (size_t)max_tiles(lat->g);
-  alloc((void**)&lat->pdone, ncount * sizeof(unsigned));
   alloc((void**)&lat->err, sizeof(int));
-  if (e == cudaSuccess) e = cudaMemset(lat->pdone, 0, ncount * sizeof(unsigned));
   if (e == cudaSuccess)
     e = cudaMemset(lat->psi, 0, (size_t)psi_elems(lat->g) * real_bytes(storage));
   if (e == cudaSuccess) e = cudaMemset(lat->err, 0, sizeof(int));
@@ -491,7 +467,6 @@ mlbm_status mlbm_lattice_destroy(mlbm_lattice* lat) {
   cudaFree(lat->nbw);
   cudaFree(lat->staging);
   cudaFree(lat->stats_scratch);
-  cudaFree(lat->pdone);
   cudaFree(lat->err);
   compact_free(lat);
   delete lat;
@@ -818,7 +793,8 @@ mlbm_status mlbm_plane_profile(mlbm_lattice* lat, int64_t* n_fluid_x,
 
 mlbm_status mlbm_set_step_kernel(mlbm_lattice* lat, int32_t kind) {
   if (mlbm_status st = check_lat(lat)) return st;
-  if (kind < MLBM_KERNEL_AUTO || kind > MLBM_KERNEL_BAND)
+  if (kind != MLBM_KERNEL_AUTO && kind != MLBM_KERNEL_TWO_PASS &&
+      kind != MLBM_KERNEL_COMPACT && kind != MLBM_KERNEL_BAND)
     return fail(MLBM_ERR_ARG, "invalid step kernel %d", kind);
   if (kind == MLBM_KERNEL_BAND &&
       !compact_band_supported(lat, lat->compact.band_rows))
@@ -826,35 +802,11 @@ mlbm_status mlbm_set_step_kernel(mlbm_lattice* lat, int32_t kind) {
                 "one-pass step needs FP32 or FP16 storage, at most 2048 x 2048 "
                 "x 1024 nodes, a whole lattice (not a slab) and bands that "
                 "fit shared memory");
-  if (kind == MLBM_KERNEL_FUSED && !lat->fused.ok)
-    return fail(MLBM_ERR_ARG, "fused kernel does not fit this lattice");
-  if ((kind == MLBM_KERNEL_COMPACT || kind == MLBM_KERNEL_WAVE) &&
-      !lat->compact.two_pass_ok)
+  if (kind == MLBM_KERNEL_COMPACT && !lat->compact.two_pass_ok)
     return fail(MLBM_ERR_ARG,
                 "compact kernels need FP32 or FP16 storage and at most "
                 "2048 x 2048 x 1024 nodes");
-  if (kind == MLBM_KERNEL_SINGLE_PASS && !lat->compact.supported)
-    return fail(MLBM_ERR_ARG,
-                "single-pass step needs FP32 or FP16 storage, ly and lz >= 4 "
-                "and a row that fits shared memory");
   lat->step_kernel = kind;
-  return MLBM_OK;
-}
-
-mlbm_status mlbm_set_tuning(mlbm_lattice* lat, int32_t rows_per_item,
-                            int32_t plane_lag) {
-  if (mlbm_status st = check_lat(lat)) return st;
-  if (rows_per_item < 0 || plane_lag < 0 || rows_per_item > 16 ||
-      (rows_per_item & (rows_per_item - 1)) != 0 || plane_lag > 64)
-    return fail(MLBM_ERR_ARG, "invalid tuning (rows 0 or 1..16 power of two, lag 0..64)");
-  DeviceGuard restore_device;
-  if (mlbm_status st = activate(lat)) return st;
-  // the progress counters count this tiling's planes: restart them
-  CUDA_TRY(cudaStreamSynchronize(lat->stream), "tuning sync");
-  CUDA_TRY(cudaMemset(lat->pdone, 0, sizeof(unsigned) * max_tiles(lat->g)),
-           "counter reset");
-  lat->fused = fused_shape(lat->g, lat->storage, rows_per_item, plane_lag);
-  lat->fused_epoch = 0;
   return MLBM_OK;
 }
 
@@ -873,6 +825,22 @@ int32_t mlbm_get_step_kernel(const mlbm_lattice* lat) {
   return lat ? effective_kernel(lat) : -1;
 }
 
+mlbm_status mlbm_set_wait_limit(mlbm_lattice* lat, uint64_t ns) {
+  if (mlbm_status st = check_lat(lat)) return st;
+  lat->wait_ns = ns ? ns : kDefaultWaitNs;
+  return MLBM_OK;
+}
+
+mlbm_status mlbm_test_stall_wait(mlbm_lattice* lat) {
+  if (mlbm_status st = check_lat(lat)) return st;
+  if (effective_kernel(lat) != MLBM_KERNEL_BAND)
+    return fail(MLBM_ERR_STATE,
+                "test_stall_wait: the lattice's step kernel has no such wait "
+                "(select MLBM_KERNEL_BAND)");
+  lat->stall_test = true;
+  return MLBM_OK;
+}
+
 mlbm_status mlbm_set_band_shape(mlbm_lattice* lat, int32_t rows,
                                 int32_t planes) {
   if (mlbm_status st = check_lat(lat)) return st;
@@ -880,29 +848,6 @@ mlbm_status mlbm_set_band_shape(mlbm_lattice* lat, int32_t rows,
     return fail(MLBM_ERR_ARG, "invalid one-pass shape %d rows x %d planes",
                 rows, planes);
   return compact_set_band_shape(lat, rows, planes);
-}
-
-mlbm_status mlbm_set_wave_shape(mlbm_lattice* lat, int32_t tile_nodes,
-                                int32_t lookahead) {
-  if (mlbm_status st = check_lat(lat)) return st;
-  if (tile_nodes < 32 || tile_nodes > 65536 || lookahead < 0 || lookahead > 256)
-    return fail(MLBM_ERR_ARG, "invalid wavefront shape %d nodes, %d planes ahead",
-                tile_nodes, lookahead);
-  DeviceGuard restore_device;
-  if (mlbm_status st = activate(lat)) return st;
-  CUDA_TRY(cudaStreamSynchronize(lat->stream), "wavefront shape");
-  return compact_set_wave_shape(lat, tile_nodes, lookahead);
-}
-
-mlbm_status mlbm_set_compact_shape(mlbm_lattice* lat, int32_t rows,
-                                   int32_t planes) {
-  if (mlbm_status st = check_lat(lat)) return st;
-  if (rows < 2 || rows > 64 || planes < 2 || planes > 4096)
-    return fail(MLBM_ERR_ARG, "invalid compact shape %d x %d", rows, planes);
-  DeviceGuard restore_device;
-  if (mlbm_status st = activate(lat)) return st;
-  CUDA_TRY(cudaStreamSynchronize(lat->stream), "compact shape");
-  return compact_set_shape(lat, rows, planes);
 }
 
 mlbm_status mlbm_autotune(mlbm_lattice* lat, int64_t step0,
@@ -919,41 +864,29 @@ mlbm_status mlbm_autotune(mlbm_lattice* lat, int64_t step0,
     if (steps_done) *steps_done = 0;
     return MLBM_OK;
   }
-  const bool compact = effective_kernel(lat) == MLBM_KERNEL_SINGLE_PASS;
-  const bool wave = effective_kernel(lat) == MLBM_KERNEL_WAVE;
+  const bool band = effective_kernel(lat) == MLBM_KERNEL_BAND;
   const int rows_u[] = {1, 2, 4, 8};
   const int planes_u[] = {2, 4, 8, 16, 32};
-  const int rows_k[] = {2, 3, 4, 6, 8};
-  const int planes_k[] = {4, 8, 16, 32};
-  // wavefront: nodes per work item x planes of lookahead
-  const int tile_w[] = {256, 512, 1024, 2048};
-  const int ahead_w[] = {1, 2, 4, 8, 16};
-  const int* rows_c = wave ? tile_w : compact ? rows_k : rows_u;
-  const int* planes_c = wave ? ahead_w : compact ? planes_k : planes_u;
-  const int nr = wave ? 4 : compact ? 5 : 4, np = wave ? 5 : compact ? 4 : 5;
+  // one-pass step: rows per band x planes per chunk
+  const int rows_b[] = {2, 4, 6, 8};
+  const int planes_b[] = {8, 16, 24, 32, 48};
+  const int* rows_c = band ? rows_b : rows_u;
+  const int* planes_c = band ? planes_b : planes_u;
+  const int nr = 4, np = 5;
   cudaEvent_t e0, e1;
   CUDA_TRY(cudaEventCreate(&e0), "autotune");
   CUDA_TRY(cudaEventCreate(&e1), "autotune");
   float best = 1e30f;
-  int br = wave ? lat->compact.wave_tile : compact ? lat->compact.rows : lat->zm.By;
-  int bp = wave ? lat->compact.wave_lookahead
-                : compact ? lat->compact.planes : lat->zm.Dz;
+  int br = band ? lat->compact.band_rows : lat->zm.By;
+  int bp = band ? lat->compact.band_planes : lat->zm.Dz;
   auto apply = [&](int r, int pl) -> mlbm_status {
-    if (wave) {
-      CUDA_TRY(cudaStreamSynchronize(lat->stream), "autotune");
-      return compact_set_wave_shape(lat, r, pl);
-    }
-    if (compact) {
-      CUDA_TRY(cudaStreamSynchronize(lat->stream), "autotune");
-      return compact_set_shape(lat, r, pl);
-    }
+    if (band) return compact_set_band_shape(lat, r, pl);
     return setup_update(lat, r, pl);
   };
   int64_t step = step0;
   for (int ri = 0; ri < nr; ++ri)
     for (int pi = 0; pi < np; ++pi) {
       const int r = rows_c[ri], pl = planes_c[pi];
-      if (compact && (lat->g.ly < 2 * r || lat->g.lz < 2 * pl)) continue;
       if (apply(r, pl) != MLBM_OK) continue;
       if (mlbm_status st = mlbm_iterate(lat, step, 1, 1, 0, 0)) return st;
       step += 1;

@@ -232,7 +232,6 @@ mlbm_status mlbm_step_pass(mlbm_lattice* lat, int64_t step, int32_t pass,
   else
     st = launch_compact_pass<__half>(lat, a, pass, wu, pass == 0);
   if (st) return st;
-  lat->compact.parts_valid = false;
   if (pass == 1) {
     lat->phase ^= 1;
     if (wu) lat->vel_valid = true;

@@ -52,8 +52,8 @@ def test_band_limits():
         lat.set_band_shape(0, 4)
     with pytest.raises(capi.MlbmError):
         lat.set_band_shape(4, 0)
-    # 65 rows of 2000 nodes: four psi planes of 67 x 2002 floats exceed
-    # shared memory
+    # 65 rows of 2000 nodes: the ring's psi planes of 67 x 2002 floats
+    # exceed shared memory
     wide = capi.Lattice((2000, 130, 2))
     with pytest.raises(capi.MlbmError):
         wide.set_band_shape(64, 2)
@@ -140,9 +140,9 @@ def test_band_large_lattice_many_blocks():
 
 
 def test_band_switching():
-    """band -> two-pass -> compact -> band -> wave -> band against two-pass
-    throughout, with odd step counts so each switch meets the other AA
-    phase."""
+    """band -> two-pass -> compact -> band -> two-pass -> band against
+    two-pass throughout, with odd step counts so each switch meets the other
+    AA phase."""
     from multiphase_lbm_b200 import capi
     shape = (64, 40, 36)
     fluid, rho = sphere_case(shape, seed=2, rmin=2.0, rmax=4.0, porosity=0.6,
@@ -152,10 +152,40 @@ def test_band_switching():
     step = 0
     for kind, n in ((capi.KERNEL_BAND, 11), (capi.KERNEL_TWO_PASS, 5),
                     (capi.KERNEL_COMPACT, 3), (capi.KERNEL_BAND, 6),
-                    (capi.KERNEL_WAVE, 7), (capi.KERNEL_BAND, 4)):
+                    (capi.KERNEL_TWO_PASS, 7), (capi.KERNEL_BAND, 4)):
         a.set_step_kernel(kind)
         a.iterate(step, n)
         b.iterate(step, n)
         step += n
     assert np.array_equal(a.field("rho"), b.field("rho"))
     assert np.array_equal(a.field("f"), b.field("f"))
+
+
+def test_band_wait_limit_runs_out_and_the_context_recovers():
+    """A hand-over wait that nothing completes (mlbm_test_stall_wait) ends
+    after the wait limit with MLBM_ERR_TIMEOUT instead of hanging; the
+    device stays usable and the lattice, initialised again, gives what a
+    fresh lattice gives."""
+    from multiphase_lbm_b200 import capi
+    shape = (48, 40, 36)
+    fluid, rho = sphere_case(shape, seed=4, rmin=2.0, rmax=4.0, porosity=0.6,
+                             rho0=1.9, amp=0.02)
+    lat = _lattice(capi, shape, fluid, rho, capi.KERNEL_BAND, **DRAIN)
+    lat.set_wait_limit(2_000_000)  # 2 ms
+    lat.iterate(0, 3)  # from AA phase 0 the first step is a two-pass step
+    lat.synchronize()
+    lat.test_stall_wait()
+    lat.iterate(3, 1)
+    with pytest.raises(capi.MlbmError) as exc:
+        lat.synchronize()
+    assert exc.value.status == 5  # MLBM_ERR_TIMEOUT
+    lat.set_wait_limit(0)
+    lat.initialize()
+    lat.iterate(0, 9)
+    ref = _lattice(capi, shape, fluid, rho, capi.KERNEL_BAND, **DRAIN)
+    ref.iterate(0, 9)
+    assert np.array_equal(lat.field("rho"), ref.field("rho"))
+    assert np.array_equal(lat.field("f"), ref.field("f"))
+    with pytest.raises(capi.MlbmError):
+        _lattice(capi, shape, fluid, rho, capi.KERNEL_COMPACT,
+                 **DRAIN).test_stall_wait()

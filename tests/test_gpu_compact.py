@@ -1,13 +1,11 @@
 """The kernels over the compact (fluid-only) population layout.
 
 COMPACT runs the two passes of the dense kernels over the compact layout and
-must match them bit for bit.  SINGLE_PASS has the same collision but forms
-psi of the next step from fixed-point part sums of the post-collision
-populations instead of a second pass, so it agrees with the reference's
-kernels (the oracle) to rounding.  Tolerances (the FP32 parity bar): density
-within 1e-5 relative pointwise, populations and velocity within 1e-5 relative
-to their largest value, over the first 100 steps; FP16 storage: density
-within 2e-3 relative.
+BAND does both in one launch with two population buffers; both must match
+the dense two-pass kernels bit for bit, and the reference's kernels (the
+oracle) to the FP32 parity bar: density within 1e-5 relative pointwise,
+populations and velocity within 1e-5 relative to their largest value, over
+the first 100 steps.
 """
 import numpy as np
 import pytest
@@ -21,18 +19,16 @@ DRAIN = dict(G=-5.0, rhos=0.223144, tau=1.0, inlet_width=3, outlet_width=1,
              rho_inlet=0.17, rho_outlet=1.90)
 
 
-def _lattice(capi, shape, fluid, rho, kernel, storage=0, shape_kc=None, **kw):
+def _lattice(capi, shape, fluid, rho, kernel, storage=0, **kw):
     lat = capi.Lattice(shape, storage=storage)
     lat.set_step_kernel(kernel)
-    if shape_kc:
-        lat.set_compact_shape(*shape_kc)
     lat.set_params(capi.default_params(**kw))
     lat.upload(fluid, rho)
     lat.initialize()
     return lat
 
 
-KINDS = [3, 4]  # KERNEL_COMPACT, KERNEL_SINGLE_PASS
+KINDS = [3, 6]  # KERNEL_COMPACT, KERNEL_BAND
 
 
 @pytest.mark.parametrize("kind", KINDS)
@@ -59,31 +55,6 @@ def test_compact_matches_oracle_drainage_100_steps(kind):
     assert e <= 1e-5, f"velocity {e:.3e}"
 
 
-# lattice shapes x compact tilings: uneven splits, exactly two tiles along y
-# or z, rows longer than one mask word, odd row lengths
-CASES = [((40, 32, 24), (4, 8)), ((33, 5, 7), (2, 2)), ((70, 9, 4), (4, 2)),
-         ((100, 12, 13), (3, 5)), ((48, 16, 16), (8, 8)), ((300, 6, 6), (3, 3))]
-
-
-@pytest.mark.parametrize("shape,kc", CASES)
-def test_single_pass_agrees_with_two_pass(shape, kc):
-    from multiphase_lbm_b200 import capi
-    fluid, rho = sphere_case(shape, seed=sum(shape), rmin=1.5, rmax=3.5,
-                             porosity=0.6, rho0=0.7, amp=0.1)
-    kw = dict(G=-5.0, rhos=0.223144, tau=1.0)
-    a = _lattice(capi, shape, fluid, rho, capi.KERNEL_SINGLE_PASS, shape_kc=kc,
-                 **kw)
-    b = _lattice(capi, shape, fluid, rho, capi.KERNEL_TWO_PASS, **kw)
-    m = fluid.astype(bool)
-    for s0, n in ((0, 1), (1, 2), (3, 47)):
-        a.iterate(s0, n)
-        b.iterate(s0, n)
-        e = pointwise_rel_err(a.field("rho"), b.field("rho"), m)
-        assert e <= 1e-5, f"{shape} {kc} step {s0 + n}: rho {e:.3e}"
-        e = rel_err(a.field("f"), b.field("f"), m)
-        assert e <= 1e-5, f"{shape} {kc} step {s0 + n}: populations {e:.3e}"
-
-
 @pytest.mark.parametrize("storage", [0, 1])
 @pytest.mark.parametrize("shape", [(40, 32, 24), (33, 5, 7), (70, 3, 2),
                                    (300, 6, 6), (1, 9, 8)])
@@ -107,91 +78,55 @@ def test_compact_two_pass_bit_identical(shape, storage):
         assert np.array_equal(u, v)
 
 
-def test_single_pass_fp16_close_to_two_pass_fp16():
-    from multiphase_lbm_b200 import capi
-    shape = (48, 40, 32)
-    fluid, rho = sphere_case(shape, seed=4, rmin=2.0, rmax=5.0, porosity=0.55,
-                             rho0=1.9, amp=0.02)
-    kw = dict(DRAIN, rho_shift=1.0)
-    a = _lattice(capi, shape, fluid, rho, capi.KERNEL_SINGLE_PASS,
-                 storage=capi.STORE_F16, **kw)
-    b = _lattice(capi, shape, fluid, rho, capi.KERNEL_TWO_PASS,
-                 storage=capi.STORE_F16, **kw)
-    a.iterate(0, 100)
-    b.iterate(0, 100)
-    m = fluid.astype(bool)
-    e = pointwise_rel_err(a.field("rho"), b.field("rho"), m)
-    assert e <= 2e-3, f"fp16 rho {e:.3e}"
-
-
-def test_single_pass_deterministic_bitwise():
-    from multiphase_lbm_b200 import capi
-    shape = (64, 32, 32)
-    fluid, rho = sphere_case(shape, seed=9, rmin=2.0, rmax=5.0, porosity=0.5,
-                             rho0=0.7, amp=0.05)
-    outs = []
-    for _ in range(2):
-        lat = _lattice(capi, shape, fluid, rho, capi.KERNEL_SINGLE_PASS,
-                       G=-6.0, rhos=0.182322)
-        lat.iterate(0, 60)
-        outs.append((lat.field("rho"), lat.field("f")))
-    assert np.array_equal(outs[0][0], outs[1][0])
-    assert np.array_equal(outs[0][1], outs[1][1])
-
-
 def test_kernel_switching_keeps_the_state():
-    """single-pass -> two-pass -> compact -> single-pass -> fused, against
-    two-pass throughout."""
+    """band -> two-pass -> compact -> band -> two-pass, against two-pass
+    throughout: the state moves between the layouts and buffers exactly."""
     from multiphase_lbm_b200 import capi
     shape = (40, 24, 20)
     fluid, rho = sphere_case(shape, seed=2, rmin=2.0, rmax=4.0, porosity=0.6,
                              rho0=1.9, amp=0.02)
-    a = _lattice(capi, shape, fluid, rho, capi.KERNEL_SINGLE_PASS, **DRAIN)
+    a = _lattice(capi, shape, fluid, rho, capi.KERNEL_BAND, **DRAIN)
     b = _lattice(capi, shape, fluid, rho, capi.KERNEL_TWO_PASS, **DRAIN)
     step = 0
-    for kind in (capi.KERNEL_SINGLE_PASS, capi.KERNEL_TWO_PASS,
-                 capi.KERNEL_COMPACT, capi.KERNEL_SINGLE_PASS,
-                 capi.KERNEL_FUSED):
+    for kind in (capi.KERNEL_BAND, capi.KERNEL_TWO_PASS, capi.KERNEL_COMPACT,
+                 capi.KERNEL_BAND, capi.KERNEL_TWO_PASS):
         a.set_step_kernel(kind)
         a.iterate(step, 15)
         b.iterate(step, 15)
         step += 15
-    m = fluid.astype(bool)
-    assert pointwise_rel_err(a.field("rho"), b.field("rho"), m) <= 1e-5
-    assert rel_err(a.field("f"), b.field("f"), m) <= 1e-5
+    assert np.array_equal(a.field("rho"), b.field("rho"))
+    assert np.array_equal(a.field("f"), b.field("f"))
 
 
-def test_single_pass_shape_and_autotune():
+def test_band_shape_autotune():
     from multiphase_lbm_b200 import capi
     shape = (64, 32, 32)
     fluid, rho = sphere_case(shape, seed=5, rmin=2.0, rmax=5.0, porosity=0.5,
                              rho0=1.9, amp=0.02)
-    a = _lattice(capi, shape, fluid, rho, capi.KERNEL_SINGLE_PASS, **DRAIN)
+    a = _lattice(capi, shape, fluid, rho, capi.KERNEL_BAND, **DRAIN)
     b = _lattice(capi, shape, fluid, rho, capi.KERNEL_TWO_PASS, **DRAIN)
     rows, planes, done = a.autotune(0, trial_steps=2)
-    assert 2 <= rows <= 8 and 2 <= planes <= 32 and done > 0
+    assert rows in (2, 4, 6, 8) and planes in (8, 16, 24, 32, 48) and done > 0
     b.iterate(0, done)
-    a.set_compact_shape(3, 5)          # reshaped while the state is compact
+    a.set_band_shape(3, 5)
     a.iterate(done, 10)
     b.iterate(done, 10)
-    m = fluid.astype(bool)
-    assert pointwise_rel_err(a.field("rho"), b.field("rho"), m) <= 1e-5
-    with pytest.raises(capi.MlbmError):
-        a.set_compact_shape(1, 8)      # tiles need two rows at least
+    assert np.array_equal(a.field("rho"), b.field("rho"))
 
 
 def test_compact_kernels_reject_what_they_cannot_run():
     from multiphase_lbm_b200 import capi
     lat = capi.Lattice((16, 16, 16), storage=capi.STORE_F64)
-    for kind in (capi.KERNEL_COMPACT, capi.KERNEL_SINGLE_PASS):
+    for kind in (capi.KERNEL_COMPACT, capi.KERNEL_BAND):
         with pytest.raises(capi.MlbmError):
             lat.set_step_kernel(kind)
     assert lat.step_kernel == capi.KERNEL_TWO_PASS       # AUTO on FP64
+    for retired in (1, 4, 5, 7):
+        with pytest.raises(capi.MlbmError):
+            lat.set_step_kernel(retired)
     lat = capi.Lattice((16, 3, 16))
-    with pytest.raises(capi.MlbmError):
-        lat.set_step_kernel(capi.KERNEL_SINGLE_PASS)     # needs ly >= 4
     lat.set_step_kernel(capi.KERNEL_COMPACT)
-    assert capi.Lattice((16, 16, 16)).step_kernel == capi.KERNEL_COMPACT
+    lat.set_step_kernel(capi.KERNEL_BAND)
 
 
 @pytest.mark.parametrize("storage", [0, 1])

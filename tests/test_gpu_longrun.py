@@ -65,11 +65,11 @@ def test_fp32_and_fp16_against_fp64_long_run():
 
 
 def test_long_run_kernels_agree_bitwise():
-    """The compact two-pass, wavefront and dense two-pass steps give the same
+    """The compact two-pass, one-pass and dense two-pass steps give the same
     bits after 3,000 steps (FP32)."""
     from multiphase_lbm_b200 import capi
     _, _, a = _run(capi.STORE_F32, capi.KERNEL_COMPACT)
-    _, _, b = _run(capi.STORE_F32, capi.KERNEL_WAVE)
+    _, _, b = _run(capi.STORE_F32, capi.KERNEL_BAND)
     _, _, c = _run(capi.STORE_F32, capi.KERNEL_TWO_PASS)
     assert np.array_equal(a, b)
     assert np.array_equal(a, c)
