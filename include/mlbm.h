@@ -283,6 +283,11 @@ mlbm_status mlbm_plane_profile(mlbm_lattice* lat, int64_t* n_fluid_x,
  *   mlbm_checkpoint_write / _read   the same through a file.
  * Slab lattices are refused (MLBM_ERR_STATE). */
 mlbm_status mlbm_checkpoint_bytes(const mlbm_lattice* lat, uint64_t* bytes);
+/* Lattice size (dims[3] = lx, ly, lz), storage and step counter of an image
+ * (any of the outputs may be NULL). */
+mlbm_status mlbm_checkpoint_info(const void* image, uint64_t bytes,
+                                 int32_t* dims, int32_t* storage,
+                                 int64_t* step);
 mlbm_status mlbm_checkpoint_save(mlbm_lattice* lat, int64_t step, void* image,
                                  uint64_t bytes);
 mlbm_status mlbm_checkpoint_load(mlbm_lattice* lat, const void* image,

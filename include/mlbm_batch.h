@@ -38,6 +38,12 @@ mlbm_status mlbm_batch_destroy(mlbm_batch* b);
 mlbm_status mlbm_batch_add(mlbm_batch* b, int32_t nx, int32_t ny, int32_t nz,
                            const mlbm_params* params, const uint8_t* is_fluid,
                            const float* rho, int64_t step0, int32_t* id);
+/* Add a domain from a checkpoint image (mlbm_checkpoint_save of a domain's
+ * lattice, or of any lattice of the batch's storage): it resumes where the
+ * image was taken, bit for bit, with the image's step counter.  Used to
+ * preempt a domain (save, remove) and resume it later. */
+mlbm_status mlbm_batch_add_checkpoint(mlbm_batch* b, const void* image,
+                                      uint64_t bytes, int32_t* id);
 /* Remove a domain and free its memory. */
 mlbm_status mlbm_batch_remove(mlbm_batch* b, int32_t id);
 /* Number of domains, and device bytes they hold. */

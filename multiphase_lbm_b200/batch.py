@@ -15,6 +15,8 @@ BATCH_SIGNATURES = [
     ("mlbm_batch_add", C.c_int, [_VP, C.c_int32, C.c_int32, C.c_int32,
                                  C.POINTER(Params), _VP, _VP, C.c_int64,
                                  C.POINTER(C.c_int32)]),
+    ("mlbm_batch_add_checkpoint", C.c_int, [_VP, _VP, C.c_uint64,
+                                            C.POINTER(C.c_int32)]),
     ("mlbm_batch_remove", C.c_int, [_VP, C.c_int32]),
     ("mlbm_batch_count", C.c_int32, [_VP]),
     ("mlbm_batch_bytes", C.c_uint64, [_VP]),
@@ -77,6 +79,19 @@ class Batch:
                                     fl.ctypes.data, r.ctypes.data, step0,
                                     C.byref(did)))
         self.shapes[did.value] = fl.shape
+        return did.value
+
+    def add_checkpoint(self, image: np.ndarray) -> int:
+        """Admit a domain from a checkpoint image (Lattice.checkpoint); it
+        resumes at the image's step, bit for bit."""
+        a = np.ascontiguousarray(image, np.uint8)
+        did = C.c_int32()
+        check(blib().mlbm_batch_add_checkpoint(self.h, a.ctypes.data, a.nbytes,
+                                               C.byref(did)))
+        dims = (C.c_int32 * 3)()
+        check(lib().mlbm_checkpoint_info(a.ctypes.data, a.nbytes, dims, None,
+                                         None))
+        self.shapes[did.value] = tuple(dims)
         return did.value
 
     def remove(self, did: int):

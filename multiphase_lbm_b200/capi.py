@@ -130,6 +130,7 @@ SIGNATURES = [
     ("mlbm_slab_ring_exchange", C.c_int, [_VP, C.c_int32]),
     ("mlbm_slab_ring_destroy", C.c_int, [_VP]),
     ("mlbm_checkpoint_bytes", C.c_int, [_VP, C.POINTER(C.c_uint64)]),
+    ("mlbm_checkpoint_info", C.c_int, [_VP, C.c_uint64, _VP, _VP, _VP]),
     ("mlbm_checkpoint_save", C.c_int, [_VP, C.c_int64, _VP, C.c_uint64]),
     ("mlbm_checkpoint_load", C.c_int, [_VP, _VP, C.c_uint64,
                                        C.POINTER(C.c_int64)]),

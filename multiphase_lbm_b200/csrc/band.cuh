@@ -42,8 +42,9 @@
 // writes the same values at other addresses.
 //
 // Neighbours that are solid contribute psi(rhos) (wall adhesion,
-// include/iteration_device.cuh:69-152); their shared-memory entries are
-// never written and never read (the node's neighbour word selects).
+// include/iteration_device.cuh:69-152): the density warps write psi(rhos)
+// at the solid positions of every ring plane, so the update reads all 18
+// neighbours from shared memory alike.
 #pragma once
 
 #include "compact2.cuh"
@@ -178,6 +179,7 @@ __global__ void __launch_bounds__(kBandThreads, 2)
   }
   __syncthreads();
 
+  const float psi_solid = psi_of<float>(p, p.rhos);
   if (threadIdx.x < kBandD) {
     // ---- density warps: planes j = 0 .. nplanes + 1 of the march --------
     const int td = threadIdx.x;
@@ -199,6 +201,20 @@ __global__ void __launch_bounds__(kBandThreads, 2)
         ra[0] = y0 - 1; rb[0] = g.ly; ra[1] = 0; rb[1] = 1; nr = 2;
       } else {
         ra[0] = y0 - 1; rb[0] = y1 + 1;
+      }
+      // psi(rhos) at the solid positions of the slot's rows (wall
+      // adhesion: a solid neighbour contributes psi(rhos))
+      for (int jr = 0; jr < rows + 2; ++jr) {
+        int yy = y0 - 1 + jr;
+        yy = yy < 0 ? yy + g.ly : (yy >= g.ly ? yy % g.ly : yy);
+        const uint2* wrow = wtab + ((long long)zw * g.ly + yy) * g.wpr;
+        float* row = slot + jr * P;
+        for (int x = td; x < g.lx; x += kBandD) {
+          if ((__ldg(&wrow[x >> 5].x) >> (x & 31)) & 1u) continue;
+          row[x + 1] = psi_solid;
+          if (x == 0) row[g.lx + 1] = psi_solid;
+          if (x == g.lx - 1) row[0] = psi_solid;
+        }
       }
       for (int r = 0; r < nr; ++r) {
         const int kf = band_row_start(wtab, g, zw, ra[r]);
@@ -245,7 +261,6 @@ __global__ void __launch_bounds__(kBandThreads, 2)
 
   // ---- update warps: plane u of the march needs march planes u, u+1, u+2 --
   const int tu = threadIdx.x - kBandD;
-  const float psi_solid = psi_of<float>(p, p.rhos);
   if (stall && blockIdx.x == 0 && !band_wait(never, 0u, wait_ns, err)) return;
   for (int u = 0; u < nplanes; ++u) {
     for (int j = u == 0 ? 0 : u + 2; j <= u + 2; ++j)
@@ -297,9 +312,7 @@ __global__ void __launch_bounds__(kBandThreads, 2)
             [&](int i) {
               const float* pl = ez(i) < 0 ? sm : (ez(i) > 0 ? spl : s0);
               const int o = ey(i) * P + ex(i);
-              const float pa = ((na.nb >> opp(i)) & 1u) ? pl[ca + o] : psi_solid;
-              const float pb = ((nbn.nb >> opp(i)) & 1u) ? pl[cb + o] : psi_solid;
-              return make_float2(pa, pb);
+              return make_float2(pl[ca + o], pl[cb + o]);
             },
             f, ux, uy, uz);
       }

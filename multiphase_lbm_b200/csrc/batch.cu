@@ -303,6 +303,27 @@ mlbm_status run_steps(mlbm_batch* b, int n, int reverse, unsigned inject) {
 
 }  // namespace
 
+namespace {
+// Put an initialised (or restored) lattice into a free slot; it joins at the
+// next iterate call with its step counter at step0.
+int32_t insert_domain(mlbm_batch* b, mlbm_lattice* lat, int64_t step0) {
+  int slot = -1;
+  for (size_t s = 0; s < b->dom.size(); ++s)
+    if (!b->dom[s]) { slot = (int)s; break; }
+  if (slot < 0) {
+    slot = (int)b->dom.size();
+    b->dom.push_back(nullptr);
+    b->origin.push_back(0);
+    b->phase_base.push_back(0);
+  }
+  b->dom[slot] = lat;
+  b->origin[slot] = b->bstep - step0;
+  b->phase_base[slot] = (lat->phase + (int)(b->bstep & 1)) & 1;
+  b->dirty = true;
+  return slot;
+}
+}  // namespace
+
 extern "C" {
 
 mlbm_status mlbm_batch_create(int32_t storage, int32_t device,
@@ -374,22 +395,38 @@ mlbm_status mlbm_batch_add(mlbm_batch* b, int32_t nx, int32_t ny, int32_t nz,
     mlbm_lattice_destroy(lat);
     return st;
   }
-  int slot = -1;
-  for (size_t s = 0; s < b->dom.size(); ++s)
-    if (!b->dom[s]) { slot = (int)s; break; }
-  if (slot < 0) {
-    slot = (int)b->dom.size();
-    b->dom.push_back(nullptr);
-    b->origin.push_back(0);
-    b->phase_base.push_back(0);
-  }
-  b->dom[slot] = lat;
-  b->origin[slot] = b->bstep - step0;
-  b->phase_base[slot] = (lat->phase + (int)(b->bstep & 1)) & 1;
-  b->dirty = true;
-  *id = slot;
+  *id = insert_domain(b, lat, step0);
   return MLBM_OK;
 }
+
+mlbm_status mlbm_batch_add_checkpoint(mlbm_batch* b, const void* image,
+                                      uint64_t bytes, int32_t* id) {
+  if (!b || !image || !id) return bfail(MLBM_ERR_ARG, "null argument");
+  int32_t dims[3], storage;
+  int64_t step0 = 0;
+  if (mlbm_status st = mlbm_checkpoint_info(image, bytes, dims, &storage, &step0))
+    return st;
+  if (storage != b->storage)
+    return bfail(MLBM_ERR_ARG, "checkpoint storage differs from the batch's");
+  mlbm::DeviceGuard restore_device;
+  BCUDA(cudaSetDevice(b->device), "cudaSetDevice");
+  mlbm_lattice* lat = nullptr;
+  if (mlbm_status st = mlbm_lattice_create(dims[0], dims[1], dims[2], b->storage,
+                                           b->device, &lat))
+    return st;
+  mlbm_status st = mlbm_set_stream(lat, b->stream);
+  if (!st)
+    st = mlbm_set_step_kernel(lat, lat->compact.two_pass_ok ? MLBM_KERNEL_COMPACT
+                                                           : MLBM_KERNEL_TWO_PASS);
+  if (!st) st = mlbm_checkpoint_load(lat, image, bytes, &step0);
+  if (st) {
+    mlbm_lattice_destroy(lat);
+    return st;
+  }
+  *id = insert_domain(b, lat, step0);
+  return MLBM_OK;
+}
+
 
 mlbm_status mlbm_batch_remove(mlbm_batch* b, int32_t id) {
   if (!b || id < 0 || id >= (int)b->dom.size() || !b->dom[id])

@@ -126,6 +126,28 @@ mlbm_status mlbm_checkpoint_bytes(const mlbm_lattice* lat, uint64_t* bytes) {
   return MLBM_OK;
 }
 
+mlbm_status mlbm_checkpoint_info(const void* image, uint64_t bytes,
+                                 int32_t* dims, int32_t* storage,
+                                 int64_t* step) {
+  if (!image) return set_error(MLBM_ERR_ARG, "checkpoint: null argument");
+  if (bytes < sizeof(CkptHeader))
+    return set_error(MLBM_ERR_ARG, "checkpoint: image is truncated");
+  CkptHeader h;
+  std::memcpy(&h, image, sizeof h);
+  if (std::memcmp(h.magic, kMagic, 8) != 0)
+    return set_error(MLBM_ERR_ARG, "checkpoint: not a checkpoint image");
+  if (h.version != kVersion || h.header_bytes != sizeof(CkptHeader))
+    return set_error(MLBM_ERR_ARG, "checkpoint: unsupported format version");
+  if (dims) {
+    dims[0] = h.lx;
+    dims[1] = h.ly;
+    dims[2] = h.lz;
+  }
+  if (storage) *storage = h.storage;
+  if (step) *step = h.step;
+  return MLBM_OK;
+}
+
 mlbm_status mlbm_checkpoint_save(mlbm_lattice* lat, int64_t step, void* image,
                                  uint64_t bytes) {
   if (!lat || !image) return set_error(MLBM_ERR_ARG, "checkpoint: null argument");

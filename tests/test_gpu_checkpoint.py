@@ -98,3 +98,35 @@ def test_refuses_foreign_truncated_and_corrupted_images():
         capi.Lattice(SHAPE).checkpoint(0)  # not initialised
     a.close()
     b.close()
+
+
+@pytest.mark.parametrize("storage", [0, 1])
+def test_batch_domain_preempted_and_resumed(storage):
+    """Preemption in a batch: a domain saved (Lattice.checkpoint of the
+    domain's lattice) and removed after 7 steps, the batch advanced without
+    it, then the image admitted again (mlbm_batch_add_checkpoint) and run 9
+    more steps, ends bit-identical to the domain run 16 steps alone."""
+    from multiphase_lbm_b200 import batch, capi
+    shapes = [(40, 32, 24), (48, 40, 36)]
+    cases = [sphere_case(s, seed=20 + i, rmin=2.0, rmax=4.5, porosity=0.55,
+                         rho0=1.9, amp=0.05) for i, s in enumerate(shapes)]
+    p = capi.default_params(**DRAIN)
+    b = batch.Batch(storage)
+    ids = [b.add(fl, rho, p) for fl, rho in cases]
+    b.iterate(7)
+    b.synchronize()
+    image = b.lattice(ids[0]).checkpoint(b.domain_step(ids[0]))
+    b.remove(ids[0])
+    b.iterate(5)
+    did = b.add_checkpoint(image)
+    assert b.domain_step(did) == 7
+    b.iterate(9)
+    b.synchronize()
+    got = b.lattice(did).field("f")
+    alone = _lattice(capi, cases[0][0], cases[0][1], storage, 0)
+    alone.iterate(0, 16)
+    assert np.array_equal(got, alone.field("f"))
+    other = _lattice(capi, cases[1][0], cases[1][1], storage, 0)
+    other.iterate(0, 21)
+    assert np.array_equal(b.lattice(ids[1]).field("f"), other.field("f"))
+    b.close()
