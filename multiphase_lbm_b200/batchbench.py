@@ -14,14 +14,14 @@ Two executions of the same steps, bit-identical results:
   * plain   -- each domain advanced by its own mlbm_iterate calls, one domain
     after the other (sequential per-domain launches), with the same two-pass
     kernels as the batch.
-A third execution, plain_compact, advances the domains one after the other
-with the compact single-pass step (one launch per step and domain; results
-equal to rounding, not bit for bit).
-Both are timed with CUDA events over `--steps` steps (a bounded sample of the
-5,000-step run); solves/s = domains / (time for `--solve-steps` steps),
-extrapolated from the sample at the measured per-step rate.
+Two more executions advance the domains one after the other with the
+fluid-only kernels: plain_compact (the compact two-pass step, two launches
+per step and domain) and plain_band (the one-pass step, one launch per step
+and domain); both bit-identical to the batch.
+All are timed with CUDA events over `--steps` steps (default 5,000, the
+configured run); solves/s = domains / (time for 5,000 steps).
 
-Run: python -m multiphase_lbm_b200.batchbench [--domains 512 --steps 100]
+Run: python -m multiphase_lbm_b200.batchbench [--domains 512 --steps 5000]
 (N GPUs: torchrun --nproc-per-node N -m multiphase_lbm_b200.batchbench; every
 rank advances its share of the domains, shard.partition.)
 """
@@ -129,6 +129,7 @@ def run(ndomains=512, steps=100, storage=capi.STORE_F16, solve_steps=5000,
 
     ms_p, wall_p = plain(capi.KERNEL_TWO_PASS)
     ms_c, wall_c = plain(capi.KERNEL_COMPACT) if compact else (None, None)
+    ms_band, wall_band = plain(capi.KERNEL_BAND) if compact else (None, None)
 
     nodes = nodes_all  # whole-job throughputs below
     res = {
@@ -142,9 +143,14 @@ def run(ndomains=512, steps=100, storage=capi.STORE_F16, solve_steps=5000,
         "batched_solves_per_s": round(ndomains / (ms_b * solve_steps / 1e3), 4),
         "plain_solves_per_s": round(ndomains / (ms_p * solve_steps / 1e3), 4),
         "speedup": round(ms_p / ms_b, 3),
-        "wall_s": {"batched": round(wall_b, 2), "plain": round(wall_p, 2)},
+        "form": "batching",
+        "wall_s": {"batched": round(wall_b, 2), "plain": round(wall_p, 2),
+                   "plain_compact": None if wall_c is None else round(wall_c, 2),
+                   "plain_band": None if wall_band is None else round(wall_band, 2)},
         "plain_compact_ms_per_step": None if ms_c is None else round(ms_c, 4),
         "speedup_vs_plain_compact": None if ms_c is None else round(ms_c / ms_b, 3),
+        "plain_band_ms_per_step": None if ms_band is None else round(ms_band, 4),
+        "speedup_vs_plain_band": None if ms_band is None else round(ms_band / ms_b, 3),
         "tuning": tuning, "device_bytes": mem,
     }
     return res
@@ -153,7 +159,7 @@ def run(ndomains=512, steps=100, storage=capi.STORE_F16, solve_steps=5000,
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
     ap.add_argument("--domains", type=int, default=512)
-    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--steps", type=int, default=5000)
     ap.add_argument("--storage", default="f16", choices=["f16", "f32"])
     ap.add_argument("--seed", type=int, default=3)
     a = ap.parse_args(argv)
