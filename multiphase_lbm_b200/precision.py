@@ -12,7 +12,14 @@ Reported for each storage format, at the end of the run:
   * mass_drift        (M_end - M_0) / M_0 with M = sum of rho over fluid
                       nodes, accumulated in FP64 on the device;
   * mass_error        |M_end - M_end_64| / M_end_64;
-plus the saturation of every format every `stat_every` steps.
+plus the saturation of every format every `stat_every` steps, and where
+the FP16 error enters (error_budget): the FP64 lattice's final populations
+stored once in FP16 with each shift and read back exactly as the kernels do
+(half(f - t_i rho0) + t_i rho0 in FP32), the resulting density error per
+node relative to rho, by phase (liquid rho > rhol_spinodal, vapour rho <
+rhog_spinodal, between), and the share of fluid nodes within that error of
+the liquid threshold -- the nodes whose classification, and so the
+saturation, FP16 storage can change.
 
 Coupling and inlet: G = -4.5 and inlet density 0.3 by default.  With the
 specified G = -6.0 (inlet 0.10) the drainage case produces NaN within a few
@@ -56,6 +63,55 @@ def interface_position(lat: capi.Lattice, inlet_width: int) -> int:
         if frac[x] >= 0.5:
             return x
     return len(frac)
+
+
+T_W = np.array([1 / 3] + [1 / 18] * 3 + [1 / 36] * 6 + [1 / 18] * 3
+               + [1 / 36] * 6)
+
+
+def error_budget(lat64: capi.Lattice, fluid, shifts=(1.0, 2.0), rhol=0.2726,
+                 rhog=0.0484, sample=4_000_000, seed=0) -> dict:
+    """One-step FP16 representation error of the FP64 lattice's state (a
+    sample of fluid nodes, computed on the GPU with torch)."""
+    import ctypes as C
+
+    import torch
+    shape = tuple(fluid.shape)
+    n = int(np.prod(shape))
+    f = torch.empty((n, 19), dtype=torch.float64, device="cuda")
+    capi.check(capi.lib().mlbm_download_field_device(
+        lat64.h, capi.FIELD_POPULATIONS, capi.DTYPE_F64, C.c_void_p(f.data_ptr())))
+    torch.cuda.synchronize()
+    idx = np.flatnonzero(fluid.reshape(-1))
+    rng = np.random.default_rng(seed)
+    if len(idx) > sample:
+        idx = np.sort(rng.choice(idx, sample, replace=False))
+    f = f[torch.from_numpy(idx).cuda()]
+    f32 = f.to(torch.float32)
+    rho = f32.double().sum(1)
+    w = torch.tensor(T_W, dtype=torch.float32, device="cuda")
+    phases = {"liquid": rho > rhol, "vapour": rho < rhog,
+              "between": (rho >= rhog) & (rho <= rhol)}
+    out = {"sample_nodes": int(len(idx)),
+           "phase_share": {k: round(float(v.double().mean()), 4)
+                           for k, v in phases.items()}}
+    for shift in shifts:
+        s32 = (w * float(shift)).to(torch.float32)
+        back = (f32 - s32).to(torch.float16).to(torch.float32) + s32
+        drho = (back.double() - f32.double()).sum(1)
+        rel = (drho.abs() / rho.abs().clamp_min(1e-30))
+        per = {}
+        for k, m in phases.items():
+            if int(m.sum()) == 0:
+                continue
+            r = rel[m]
+            per[k] = {"mean_rel_rho_error": float(r.mean()),
+                      "p99_rel_rho_error": float(torch.quantile(
+                          r[:min(len(r), 1 << 24)].float(), 0.99))}
+        near = ((rho - rhol).abs() <= drho.abs()).double().mean()
+        out[f"shift_{shift:g}"] = {"per_phase": per,
+                                   "share_within_error_of_rhol": float(near)}
+    return out
 
 
 def run(shape=(384, 384, 384), steps=10000, stat_every=500, seed=384,
@@ -122,6 +178,8 @@ def run(shape=(384, 384, 384), steps=10000, stat_every=500, seed=384,
             "mass_error": abs(s["mass"] - s64["mass"]) / s64["mass"],
             "saturation_curve": curves[k],
         }
+    report["error_budget"] = error_budget(
+        lats["f64"], fluid, shifts=(1.0, rho_init, 0.5 * (rho_init + rho_inlet)))
     for lat in lats.values():
         lat.close()
     return report
@@ -146,9 +204,11 @@ def main(argv=None) -> int:
     if a.out:
         with open(a.out, "w") as fh:
             fh.write(text)
-    print(json.dumps({k: {kk: vv for kk, vv in v.items()
-                          if kk != "saturation_curve"}
-                      for k, v in rep["formats"].items()}))
+    print(json.dumps({"form": "precision",
+                      "formats": {k: {kk: vv for kk, vv in v.items()
+                                      if kk != "saturation_curve"}
+                                  for k, v in rep["formats"].items()},
+                      "error_budget": rep["error_budget"]}))
     return 0
 
 
