@@ -351,7 +351,7 @@ def timed_blocks(lat, torch, step, steps, dist):
 
 def measure(capi, torch, fluid, rho, storage_name, args, local, dist,
             kernel_id):
-    """Median device time per step of one storage format."""
+    """Median device time per step (seconds) of one storage format."""
     storage = {"f32": capi.STORE_F32, "f16": capi.STORE_F16,
                "f64": capi.STORE_F64}[storage_name]
     params = capi.default_params(**phys(args.size), rho_shift=1.0)
@@ -369,7 +369,7 @@ def measure(capi, torch, fluid, rho, storage_name, args, local, dist,
     with ClockSampler(local) as clocks:
         ms, blocks, _ = timed_blocks(lat, torch, args.warmup, args.steps, dist)
     lat.close()
-    return ms / args.steps, blocks, clocks.summary(), kernel
+    return ms / 1e3 / args.steps, blocks, clocks.summary(), kernel
 
 
 def main():

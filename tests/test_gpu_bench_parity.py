@@ -36,7 +36,11 @@ import bench  # noqa: E402
 
 pytestmark = pytest.mark.gpu
 
-FP16_RHO_TOL = 2e-2
+# FP16 storage keeps 11 significant bits of f_i - t_i (rho0 = 1): a vapour
+# node at rho ~0.1 carries an absolute error of ~1e-5 per population and
+# step, a few percent of its density after 100 steps; the saturation (the
+# liquid/vapour split) is the quantity the precision budget bounds.
+FP16_RHO_TOL = 5e-2
 FP16_SAT_TOL = 1e-3
 
 
