@@ -325,16 +325,17 @@ def run_reference_arm(args, rank, world):
 
 # ---- this library ------------------------------------------------------------
 
-def timed_blocks(lat, torch, step, steps, dist):
+def timed_blocks(lat, torch, step, steps, dist, min_s=MIN_TIMED_S):
     """Blocks of `steps` steps between CUDA events on the lattice's stream
-    (the current stream), repeated until MIN_TIMED_S of device time; returns
-    (median ms per block, blocks, next step)."""
+    (the current stream), repeated until min_s seconds of device time (and
+    at least three blocks); returns (median ms per block, blocks, next
+    step)."""
     from multiphase_lbm_b200.shard import max_over_ranks
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
     times = []
     total = 0.0
-    while total < MIN_TIMED_S * 1e3 or len(times) < 3:
+    while total < min_s * 1e3 or len(times) < 3:
         if dist:
             dist.barrier()
         torch.cuda.synchronize()
@@ -367,7 +368,8 @@ def measure(capi, torch, fluid, rho, storage_name, args, local, dist,
     lat.iterate(0, args.warmup)
     torch.cuda.synchronize()
     with ClockSampler(local) as clocks:
-        ms, blocks, _ = timed_blocks(lat, torch, args.warmup, args.steps, dist)
+        ms, blocks, _ = timed_blocks(lat, torch, args.warmup, args.steps, dist,
+                                     args.min_time)
     lat.close()
     return ms / 1e3 / args.steps, blocks, clocks.summary(), kernel
 
@@ -379,6 +381,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--storage", default="f32", choices=["f32", "f16", "f64"])
+    ap.add_argument("--min-time", type=float, default=MIN_TIMED_S,
+                    help="seconds of timed blocks (profiling runs use less)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-fp16", action="store_true")
@@ -508,23 +512,39 @@ def run_e2e(capi, torch, fluid, rho, params, storage, device, steps, dist,
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
+    marks = []
+
+    def mark():
+        torch.cuda.synchronize()
+        marks.append(time.perf_counter())
+
     t0 = time.perf_counter()
     lat.upload(fl_h, rho_h)
+    mark()
     lat.initialize()
+    mark()
     sat = []
     for k in range(steps):
         lat.iterate(k, 1)
         lat.stats_async(raw[k % 2])  # device->host read of the step's stats
         done[k % 2].record()
+        if k == 0:
+            mark()  # the first step builds the fluid-only tables
         if k > 0:
             done[(k - 1) % 2].synchronize()
             sat.append(lat.stats_from_raw(raw[(k - 1) % 2])["saturation"])
     done[(steps - 1) % 2].synchronize()
     sat.append(lat.stats_from_raw(raw[(steps - 1) % 2])["saturation"])
+    mark()
     from multiphase_lbm_b200.capi import DTYPE_F32, FIELD_RHO, check, lib
     check(lib().mlbm_download_field(lat.h, FIELD_RHO, DTYPE_F32,
                                     out_h.ctypes.data))
     dt = time.perf_counter() - t0
+    edges = [t0] + marks + [t0 + dt]
+    parts = ["upload", "initialize", "first_step", "steps_after_first",
+             "download"]
+    breakdown = {k: round((b - a) * 1e3, 3)
+                 for k, a, b in zip(parts, edges[:-1], edges[1:])}
     from multiphase_lbm_b200.shard import max_over_ranks
     dt = max_over_ranks(dt)
     lat.close()
@@ -533,7 +553,7 @@ def run_e2e(capi, torch, fluid, rho, params, storage, device, steps, dist,
     stats_bytes = 8 * capi.STATS_RAW_LEN
     assert len(sat) == steps
     return {"value": round(n * world * steps / dt / 1e6, 2), "unit": "MLUPS",
-            "steps": steps,
+            "steps": steps, "breakdown_ms": breakdown,
             "h2d_bytes_per_step": int((n + 4 * n) / steps),
             "d2h_bytes_per_step": int(stats_bytes + 4 * n / steps)}
 
