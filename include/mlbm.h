@@ -189,7 +189,9 @@ mlbm_status mlbm_iterate(mlbm_lattice* lat, int64_t step0, int32_t nsteps,
  *                populations about once per step.  Bit-identical to
  *                TWO_PASS; FP32 / FP16 storage, whole lattices (not slabs),
  *                same size limits as COMPACT; a second population buffer is
- *                allocated on first use;
+ *                allocated on first use.  Where even a band of one row does
+ *                not fit shared memory (very long rows), the steps run as
+ *                COMPACT;
  *   AUTO         (default) COMPACT where supported, else TWO_PASS.
  * (Values 1, 4 and 5 belonged to step kernels this library no longer has;
  * they are refused.)  The state moves between the layouts on demand (the
@@ -202,10 +204,10 @@ mlbm_status mlbm_iterate(mlbm_lattice* lat, int64_t step0, int32_t nsteps,
 mlbm_status mlbm_set_step_kernel(mlbm_lattice* lat, int32_t kind);
 /* The kernel the next mlbm_iterate runs (AUTO resolved); -1 for NULL. */
 int32_t mlbm_get_step_kernel(const mlbm_lattice* lat);
-/* Tiling of the BAND step: bands of about `rows` rows (y, 1..64) and chunks
- * of about `planes` planes (z, 1..1024), one block per band and chunk.
- * Default 4 x 24.  MLBM_ERR_ARG when a band's ring of psi planes does not
- * fit shared memory (6 x (rows + 2) x (lx + 2) floats). */
+/* Tiling of the BAND step: bands of at most `rows` rows (y, 1..64; fewer
+ * where the staged rows would not fit shared memory) and chunks of about
+ * `planes` planes (z, 1..1024), one block per band and chunk.  Default
+ * 4 x 24. */
 mlbm_status mlbm_set_band_shape(mlbm_lattice* lat, int32_t rows,
                                 int32_t planes);
 /* Shape of the two-pass update kernel: tile rows (block = 32 x rows

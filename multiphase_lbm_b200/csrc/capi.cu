@@ -232,6 +232,8 @@ mlbm_status launch_steps(mlbm_lattice* lat, int64_t step0, int32_t nsteps,
   }
   if (compact) {
     if (mlbm_status st = compact_enter(lat)) return st;
+    // bands that do not fit shared memory: compact two-pass steps
+    if (band && !compact_band_fits(lat)) band = false;
   } else {
     if (mlbm_status st = compact_leave(lat)) return st;
   }
@@ -796,12 +798,10 @@ mlbm_status mlbm_set_step_kernel(mlbm_lattice* lat, int32_t kind) {
   if (kind != MLBM_KERNEL_AUTO && kind != MLBM_KERNEL_TWO_PASS &&
       kind != MLBM_KERNEL_COMPACT && kind != MLBM_KERNEL_BAND)
     return fail(MLBM_ERR_ARG, "invalid step kernel %d", kind);
-  if (kind == MLBM_KERNEL_BAND &&
-      !compact_band_supported(lat, lat->compact.band_rows))
+  if (kind == MLBM_KERNEL_BAND && !compact_band_supported(lat))
     return fail(MLBM_ERR_ARG,
                 "one-pass step needs FP32 or FP16 storage, at most 2048 x 2048 "
-                "x 1024 nodes, a whole lattice (not a slab) and bands that "
-                "fit shared memory");
+                "x 1024 nodes and a whole lattice (not a slab)");
   if (kind == MLBM_KERNEL_COMPACT && !lat->compact.two_pass_ok)
     return fail(MLBM_ERR_ARG,
                 "compact kernels need FP32 or FP16 storage and at most "

@@ -26,9 +26,12 @@ struct CompactState {
   uint32_t* wbase = nullptr;   // [rows * wpr + 1]
   long long cap = 0;           // cs the buffers were allocated for
   std::vector<long long> plane_start;  // [lz + 1] first compact index of each plane
+  std::vector<uint32_t> row_start;     // [lz * ly + 1] first compact index of each row
   // one-pass step (band.cuh): the second population buffer and the tiling
   void* cpop_alt = nullptr;            // [Q][cs] populations (T)
   int band_rows = 4, band_planes = 24;  // requested rows per band, planes per chunk
+  // stage size (compact slots) of the shape last launched, and its key
+  int band_slot = 0, band_slot_rows = -1, band_slot_nb = -1, band_slot_storage = -1;
 };
 
 // Bound of the step kernels' device waits, and the test switch that makes
@@ -100,6 +103,9 @@ bool compact_two_pass_supported(int lx, int ly, int lz, int storage);
 template <typename T>
 mlbm_status launch_compact_band(mlbm_lattice* lat, const StepArgs& a,
                                 bool write_u, bool write_rho);
-bool compact_band_supported(const mlbm_lattice* lat, int rows);
+bool compact_band_supported(const mlbm_lattice* lat);
+// Whether the lattice's bands fit shared memory (tables built); where they
+// do not, BAND steps run as compact two-pass steps.
+bool compact_band_fits(mlbm_lattice* lat);
 mlbm_status compact_set_band_shape(mlbm_lattice* lat, int rows, int planes);
 }  // namespace mlbm

@@ -66,6 +66,9 @@ mlbm_status build_tables(mlbm_lattice* lat) {
   c.plane_start.assign(g.lz + 1, 0);
   for (int z = 0; z <= g.lz; ++z)
     c.plane_start[z] = h[(long long)z * g.ly * g.wpr];
+  c.row_start.assign((size_t)g.lz * g.ly + 1, 0);
+  for (long long r = 0; r <= (long long)g.lz * g.ly; ++r)
+    c.row_start[r] = h[r * g.wpr];
   e = cudaMemcpy(c.wbase, h.data(), (nwords + 1) * sizeof(uint32_t),
                  cudaMemcpyHostToDevice);
   if (e != cudaSuccess) return cuda_fail(e, "compact tables");
@@ -95,6 +98,7 @@ mlbm_status build_tables(mlbm_lattice* lat) {
     }
     c.cap = c.cs;
   }
+  c.band_slot_rows = -1;  // stage sizes follow the tables
   c.built = true;
   return MLBM_OK;
 }
@@ -298,13 +302,64 @@ namespace {
 constexpr size_t kBandSmemMax = 227 * 1024;
 
 // Bands of about `rows` rows along y and chunks of about `planes` planes
-// along z; the tallest band's psi ring must fit shared memory.
+// along z.
 BandShape band_shape(const Geom& g, int rows, int planes) {
   BandShape s;
   s.nb = std::max(1, g.ly / std::max(1, rows));
   s.nc = std::max(1, g.lz / std::max(1, planes));
   s.hmax = (g.ly + s.nb - 1) / s.nb;
+  s.slot = 0;
   return s;
+}
+
+// Compact slots one stage must hold for bands of shape s: the largest
+// aligned extent of a band's rows y0 - 1 .. y1 over all bands and planes
+// (band_ranges), plus one alignment unit so a pair load at a range's end
+// stays inside the stage.
+int band_slot(const mlbm_lattice* lat, const BandShape& s, int align) {
+  const CompactState& c = lat->compact;
+  const Geom& g = lat->g;
+  long long mx = 0;
+  for (int b = 0; b < s.nb; ++b) {
+    const int y0 = (int)((long long)b * g.ly / s.nb);
+    const int y1 = (int)((long long)(b + 1) * g.ly / s.nb);
+    int ra[2], rb[2];
+    const int n = band_row_ranges(g.ly, y0, y1, ra, rb);
+    for (int z = 0; z < g.lz; ++z) {
+      long long tot = 0;
+      for (int q = 0; q < n; ++q) {
+        const long long kf = c.row_start[(size_t)z * g.ly + ra[q]];
+        const long long ke = c.row_start[(size_t)z * g.ly + rb[q]];
+        tot += (ke + align - 1) / align * align - kf / align * align;
+      }
+      mx = std::max(mx, tot);
+    }
+  }
+  return (int)(mx + align);
+}
+
+// The band shape a launch uses: the requested rows, lowered until the psi
+// ring and the stages fit shared memory (0 bands: nothing fits).
+template <typename T>
+BandShape fit_band_shape(mlbm_lattice* lat, int rows, int planes) {
+  CompactState& c = lat->compact;
+  for (int r = std::max(1, rows); r >= 1; --r) {
+    BandShape s = band_shape(lat->g, r, planes);
+    if (c.band_slot_rows == r && c.band_slot_nb == s.nb &&
+        c.band_slot_storage == lat->storage) {
+      s.slot = c.band_slot;
+    } else {
+      s.slot = band_slot(lat, s, band_align<T>());
+      c.band_slot = s.slot;
+      c.band_slot_rows = r;
+      c.band_slot_nb = s.nb;
+      c.band_slot_storage = lat->storage;
+    }
+    if (band_smem_bytes<T>(s.hmax, lat->g.lx, s.slot) <= kBandSmemMax) return s;
+  }
+  BandShape none = band_shape(lat->g, 1, planes);
+  none.nb = 0;
+  return none;
 }
 
 template <typename T, bool WR, bool WU>
@@ -338,17 +393,20 @@ mlbm_status band_smem_attr(int device, size_t smem) {
 
 }  // namespace
 
-bool compact_band_supported(const mlbm_lattice* lat, int rows) {
-  if (!lat->compact.two_pass_ok || lat->slab) return false;
-  const BandShape s = band_shape(lat->g, rows, 1);
-  return band_smem_bytes(s.hmax, lat->g.lx) <= kBandSmemMax;
+bool compact_band_supported(const mlbm_lattice* lat) {
+  return lat->compact.two_pass_ok && !lat->slab;
+}
+
+bool compact_band_fits(mlbm_lattice* lat) {
+  if (!lat->compact.built) return false;
+  const BandShape s =
+      lat->storage == MLBM_STORE_F16
+          ? fit_band_shape<__half>(lat, lat->compact.band_rows, lat->compact.band_planes)
+          : fit_band_shape<float>(lat, lat->compact.band_rows, lat->compact.band_planes);
+  return s.nb > 0;
 }
 
 mlbm_status compact_set_band_shape(mlbm_lattice* lat, int rows, int planes) {
-  if (!compact_band_supported(lat, rows))
-    return set_error(MLBM_ERR_ARG,
-                     "one-pass step: the bands' psi planes do not fit shared "
-                     "memory (fewer rows per band, or the two-pass step)");
   lat->compact.band_rows = rows;
   lat->compact.band_planes = planes;
   return MLBM_OK;
@@ -369,10 +427,10 @@ mlbm_status launch_compact_band(mlbm_lattice* lat, const StepArgs& a,
       return cuda_fail(e, "one-pass step buffer");
     }
   }
-  const BandShape s = band_shape(lat->g, c.band_rows, c.band_planes);
-  const size_t smem = band_smem_bytes(s.hmax, lat->g.lx);
-  if (smem > kBandSmemMax)
-    return set_error(MLBM_ERR_ARG, "one-pass step: band does not fit shared memory");
+  const BandShape s = fit_band_shape<T>(lat, c.band_rows, c.band_planes);
+  if (s.nb == 0)
+    return set_error(MLBM_ERR_ARG, "one-pass step: a band does not fit shared memory");
+  const size_t smem = band_smem_bytes<T>(s.hmax, lat->g.lx, s.slot);
   if (mlbm_status st = band_smem_attr<T>(lat->device, smem)) return st;
   const bool inj = inject_now(lat, a);
   const bool stall = lat->stall_test;

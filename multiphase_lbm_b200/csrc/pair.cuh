@@ -38,7 +38,7 @@
 namespace mlbm {
 
 // ---- packed FP32 -----------------------------------------------------------
-// Every packed operation is one fma.rn.f32x2 (inline PTX):
+// Every packed operation is one fma.rn.f32x2 (__ffma2_rn):
 //   a + b = fma(a, 1, b),  a - b = fma(b, -1, a),  a * b = fma(a, b, -0),
 // each exact up to its one rounding (the products with +-1 are exact, and
 // adding -0 leaves a product unchanged, signed zeros included), so every lane
@@ -53,16 +53,7 @@ static __constant__ float2 c_pk_neg_zero = {-0.f, -0.f};
 
 __device__ __forceinline__ float2 p_dup(float v) { return make_float2(v, v); }
 __device__ __forceinline__ float2 p_fma(float2 a, float2 b, float2 c) {
-  float2 d;
-  asm("{.reg .b64 ra, rb, rc, rd;\n\t"
-      "mov.b64 ra, {%2, %3};\n\t"
-      "mov.b64 rb, {%4, %5};\n\t"
-      "mov.b64 rc, {%6, %7};\n\t"
-      "fma.rn.f32x2 rd, ra, rb, rc;\n\t"
-      "mov.b64 {%0, %1}, rd;}"
-      : "=f"(d.x), "=f"(d.y)
-      : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y), "f"(c.x), "f"(c.y));
-  return d;
+  return __ffma2_rn(a, b, c);
 }
 __device__ __forceinline__ float2 p_add(float2 a, float2 b) {
   return p_fma(a, c_pk_one, b);
