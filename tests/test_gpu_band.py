@@ -52,11 +52,20 @@ def test_band_limits():
         lat.set_band_shape(0, 4)
     with pytest.raises(capi.MlbmError):
         lat.set_band_shape(4, 0)
-    # 65 rows of 2000 nodes: the ring's psi planes of 67 x 2002 floats
-    # exceed shared memory
-    wide = capi.Lattice((2000, 130, 2))
-    with pytest.raises(capi.MlbmError):
-        wide.set_band_shape(64, 2)
+
+
+
+def test_band_rows_too_long_for_shared_memory_run_as_compact():
+    """Rows of 2000 nodes: not even a band of one row (three staged rows)
+    fits shared memory, so BAND steps run as COMPACT steps -- the same bits."""
+    from multiphase_lbm_b200 import capi
+    shape = (2000, 4, 3)
+    fluid, rho = sphere_case(shape, seed=1, rmin=1.0, rmax=1.5, porosity=0.7,
+                             rho0=1.5, amp=0.2)
+    a = _run(_lattice(capi, shape, fluid, rho, capi.KERNEL_BAND, **DRAIN), 6)
+    b = _run(_lattice(capi, shape, fluid, rho, capi.KERNEL_TWO_PASS, **DRAIN), 6)
+    for u, v in zip(a, b):
+        assert np.array_equal(u, v)
 
 
 def test_band_matches_oracle_drainage_100_steps():
