@@ -241,7 +241,6 @@ mlbm_status launch_steps(mlbm_lattice* lat, int64_t step0, int32_t nsteps,
     StepArgs a{(long long)(step0 + s), reverse, inject_type};
     const bool last = s == nsteps - 1;
     const bool wu = (flags & MLBM_ITER_WRITE_VELOCITY) && last;
-    const int out = wu ? (OUT_RHO | OUT_VEL) : (last ? OUT_RHO : OUT_NONE);
     mlbm_status st;
     // the one-pass step starts and ends in AA phase 1; from phase 0 one
     // two-pass step gets there

@@ -18,7 +18,8 @@
 //
 // mbarrier waits are bounded: a wait that runs out raises the error flag;
 // the block then finishes the plane without storing and returns at the next
-// barrier, so no thread is left behind at a barrier.
+// barrier, so no thread is left behind at a barrier, after thread 0 has
+// waited (bounded again) for the copies still in flight.
 #pragma once
 
 #include <cuda.h>
@@ -120,6 +121,7 @@ __global__ void __launch_bounds__(256)
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   __syncthreads();
+  int issued_hi = z0 + 1;  // the last plane whose copy thread 0 issued
   if (tid == 0) {
     issue(z0 - 1);
     issue(z0);
@@ -142,6 +144,7 @@ __global__ void __launch_bounds__(256)
       // the last barrier) before the bulk copy overwrites it
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       issue(z + 2);
+      issued_hi = z + 2;
     }
     const int n = valid ? (int)node_index(g, x, y, z) : 0;
     const uint32_t nb = valid ? nbw[n] : 0u;
@@ -180,7 +183,14 @@ __global__ void __launch_bounds__(256)
       scatter<T, PHASE>(pop, g.plane, nbr, nb, n, shift, f);
     }
     // the slot of plane z-1 is refilled next iteration: all reads done first
-    if (__syncthreads_or(!ok)) return;
+    if (__syncthreads_or(!ok)) {
+      // a wait ran out: leave no bulk copy in flight into this block's
+      // shared memory (each ring slot's last issued plane, bounded again)
+      if (tid == 0)
+        for (int q = max(z0 - 1, issued_hi - (kRing - 1)); q <= issued_hi; ++q)
+          wait_plane(q);
+      return;
+    }
   }
 }
 
