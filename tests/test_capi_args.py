@@ -72,3 +72,23 @@ def test_async_stats_buffer_checked_in_python():
     with pytest.raises(ValueError):
         capi.Lattice.stats_async(object.__new__(capi.Lattice),
                                  np.zeros(3, np.float64))
+
+
+def test_checkpoint_entry_points_refuse_bad_arguments():
+    L = capi.lib()
+    n = C.c_uint64()
+    _refused(L.mlbm_checkpoint_bytes(None, C.byref(n)), "null argument")
+    _refused(L.mlbm_checkpoint_save(None, 0, None, 0), "null argument")
+    _refused(L.mlbm_checkpoint_load(None, None, 0, None), "null argument")
+    _refused(L.mlbm_checkpoint_write(None, 0, b"x"), "null argument")
+    _refused(L.mlbm_checkpoint_read(None, b"x", None), "null argument")
+    _refused(L.mlbm_checkpoint_info(None, 0, None, None, None), "null argument")
+    img = np.zeros(4096, np.uint8)
+    _refused(L.mlbm_checkpoint_info(img.ctypes.data, 16, None, None, None),
+             "truncated")
+    _refused(L.mlbm_checkpoint_info(img.ctypes.data, img.nbytes, None, None,
+                                    None), "not a checkpoint")
+    img[:8] = np.frombuffer(b"MLBMCKPT", np.uint8)
+    img[8:12] = np.frombuffer(np.uint32(99).tobytes(), np.uint8)
+    _refused(L.mlbm_checkpoint_info(img.ctypes.data, img.nbytes, None, None,
+                                    None), "unsupported format version")
