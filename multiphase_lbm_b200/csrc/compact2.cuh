@@ -134,21 +134,32 @@ __global__ void __launch_bounds__(kC2Threads, 5)
                                   rho_out, psi, g, p, a, inj);
 }
 
-template <typename T, int PHASE, bool WRITE_U>
+// With STATS the launch also gathers the phase statistics of the step's
+// density (stats_tap.cuh): every block writes its record into the
+// column-major partials `part` (ST_COUNT x gridDim.x), so no thread leaves
+// before the block's reduction.
+template <typename T, int PHASE, bool WRITE_U, bool STATS>
 __global__ void __launch_bounds__(kC2Threads, 3)
     k_cupdate(T* __restrict__ cpop, uint32_t cs, const uint2* __restrict__ cinfo,
               const uint2* __restrict__ wtab, int kbeg, int nfluid,
               const float* __restrict__ psi, float* __restrict__ vel, Geom g,
-              Phys p, StepArgs a, bool inj) {
+              Phys p, StepArgs a, bool inj, float low_T,
+              double* __restrict__ part) {
   const long long k = kbeg + c2_nodes_per_thread<PHASE>() *
                                  ((long long)blockIdx.x * kC2Threads + threadIdx.x);
-  if (k >= nfluid) return;
-  if (PHASE == 0)
-    node_update0<T, WRITE_U>(cpop, cs, cinfo, wtab, (int)k, PsiPlain{psi}, vel,
-                             g, p, a, inj);
-  else
-    pair_update<T, 1, WRITE_U>(cpop, cs, cinfo, wtab, (int)k, nfluid,
-                               PsiPlain{psi}, vel, g, p, a, inj);
+  StatAcc acc;
+  if (STATS) acc.clear();
+  if (k < nfluid) {
+    if (PHASE == 0)
+      node_update0<T, WRITE_U, PsiPlain, STATS>(cpop, cs, cinfo, wtab, (int)k,
+                                                PsiPlain{psi}, vel, g, p, a,
+                                                inj, low_T, &acc);
+    else
+      pair_update<T, 1, WRITE_U, PsiPlain, STATS>(cpop, cs, cinfo, wtab, (int)k,
+                                                  nfluid, PsiPlain{psi}, vel,
+                                                  g, p, a, inj, low_T, &acc);
+  }
+  if (STATS) stat_block_write<kC2Threads>(acc, part, gridDim.x);
 }
 
 }  // namespace mlbm

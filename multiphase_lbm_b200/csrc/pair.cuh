@@ -34,6 +34,7 @@
 #include "compact.cuh"
 #include "kernels.cuh"
 #include "lattice.cuh"
+#include "stats_tap.cuh"
 
 namespace mlbm {
 
@@ -232,28 +233,14 @@ __device__ __forceinline__ void collide2(const Phys& p, float2 d, float2 psi_sel
   }
 }
 
-// psi readers of the update pass, given psi_index() positions:
-//   PsiPlain    the float psi array through the read-only path (psi complete
-//               before the launch);
-//   PsiCoherent the same array with ordinary coherent loads (psi written by
-//               the same launch, wave.cuh).
+// psi reader of the update pass, given psi_index() positions: the float psi
+// array through the read-only path (psi complete before the launch).
 // ready() is called once before the first psi read.
 struct PsiPlain {
   const float* psi;
   __device__ __forceinline__ void ready() const {}
   __device__ __forceinline__ float self(uint32_t i) const { return __ldg(psi + i); }
   __device__ __forceinline__ float nb(uint32_t i, int) const { return __ldg(psi + i); }
-};
-struct PsiCoherent {
-  const float* psi;
-  __device__ __forceinline__ void ready() const {}
-  __device__ __forceinline__ float ld(uint32_t i) const {
-    float v;
-    asm volatile("ld.global.f32 %0, [%1];" : "=f"(v) : "l"(psi + i));
-    return v;
-  }
-  __device__ __forceinline__ float self(uint32_t i) const { return ld(i); }
-  __device__ __forceinline__ float nb(uint32_t i, int) const { return ld(i); }
 };
 
 // The two nodes of pair k (k even) and whether the second one exists.
@@ -331,21 +318,26 @@ __device__ __forceinline__ void pair_density(const T* cpop, uint32_t cs,
   if (q.two) store_psi<float>(psi, g, q.b.x, q.b.y, q.b.z, psi_of<float>(p, d.y));
 }
 
-// Update pass of one pair (the work of k_cupdate for two nodes).
-template <typename T, int PHASE, bool WRITE_U, class PsiR>
+// Update pass of one pair (the work of k_cupdate for two nodes).  With
+// STATS, the pair's phase statistics are folded into *acc (stats_tap.cuh):
+// the neighbour psi the force loads, compared with low_T, give the
+// liquid-boundary test.
+template <typename T, int PHASE, bool WRITE_U, class PsiR, bool STATS = false>
 __device__ __forceinline__ void pair_update(T* cpop, uint32_t cs,
                                             const uint2* __restrict__ cinfo,
                                             const uint2* __restrict__ wtab,
                                             int k, int nfluid, const PsiR& pr,
                                             float* vel, const Geom& g,
                                             const Phys& p, const StepArgs& a,
-                                            bool inj) {
+                                            bool inj, float low_T = 0.f,
+                                            StatAcc* acc = nullptr) {
   const Pair q = load_pair(cinfo, k, nfluid);
   uint32_t A[Q], B[Q];
   float2 f[Q];
   pair_load<T, PHASE>(cpop, cs, wtab, g, q, p.rho_shift, A, B, f);
   const float2 d = pair_rho(p, g, a, inj, q, f);
   float2 ux, uy, uz;
+  uint32_t lowa = 0u, lowb = 0u;  // bit i: psi of x - e_i below low_T
   {
     const uint32_t pa = (uint32_t)psi_index(g, q.a.x, q.a.y, q.a.z);
     const uint32_t pb = (uint32_t)psi_index(g, q.b.x, q.b.y, q.b.z);
@@ -355,7 +347,12 @@ __device__ __forceinline__ void pair_update(T* cpop, uint32_t cs,
         p, d, make_float2(pr.self(pa), pr.self(pb)),
         [&](int i) {
           const int o = ex(i) + ey(i) * sy + ez(i) * sz;
-          return make_float2(pr.nb(pa + o, i), pr.nb(pb + o, i));
+          const float va = pr.nb(pa + o, i), vb = pr.nb(pb + o, i);
+          if (STATS) {  // x + e_i is x - e_opp(i)
+            lowa |= (va < low_T ? 1u : 0u) << opp(i);
+            lowb |= (vb < low_T ? 1u : 0u) << opp(i);
+          }
+          return make_float2(va, vb);
         },
         f, ux, uy, uz);
   }
@@ -380,6 +377,10 @@ __device__ __forceinline__ void pair_update(T* cpop, uint32_t cs,
     vel[3 * nb + 2] = uz.y;
   }
   pair_scatter<T, PHASE>(cpop, cs, k, A, B, p.rho_shift, f);
+  if (STATS) {
+    acc->add(p, d.x, q.a.nb, lowa);
+    if (q.two) acc->add(p, d.y, q.b.nb, lowb);
+  }
 }
 
 
@@ -417,13 +418,15 @@ __device__ __forceinline__ void node_density0(const T* cpop, uint32_t cs,
   store_psi<float>(psi, g, n.x, n.y, n.z, psi_of<float>(p, d));
 }
 
-template <typename T, bool WRITE_U, class PsiR>
+template <typename T, bool WRITE_U, class PsiR, bool STATS = false>
 __device__ __forceinline__ void node_update0(T* cpop, uint32_t cs,
                                              const uint2* __restrict__ cinfo,
                                              const uint2* __restrict__ wtab,
                                              int k, const PsiR& pr, float* vel,
                                              const Geom& g, const Phys& p,
-                                             const StepArgs& a, bool inj) {
+                                             const StepArgs& a, bool inj,
+                                             float low_T = 0.f,
+                                             StatAcc* acc = nullptr) {
   const PairNode n = pair_node(cinfo, k);
   if (!(n.nb & NB_SELF)) return;
   const float shift = p.rho_shift;
@@ -431,8 +434,14 @@ __device__ __forceinline__ void node_update0(T* cpop, uint32_t cs,
   aa_addresses0(wtab, g, cs, n, A);
   float f[Q];
   float ux = 0.f, uy = 0.f, uz = 0.f;
+  float dn;          // the node's density (statistics)
+  uint32_t low = 0u;  // bit i: psi of x - e_i below low_T
   if (n.kind) {
-    slab_populations<float>(slab_density(p, n.kind), f);
+    dn = slab_density(p, n.kind);
+    slab_populations<float>(dn, f);
+    // a slab node loads no neighbour psi: the liquid test reads them here
+    if (STATS && dn > p.rhol_spinodal)
+      low = stat_low_bits(pr.psi, g, n.x, n.y, n.z, low_T);
   } else {
 #pragma unroll
     for (int e = 0; e < Q; ++e)
@@ -441,12 +450,17 @@ __device__ __forceinline__ void node_update0(T* cpop, uint32_t cs,
 #pragma unroll
     for (int i = 0; i < Q; ++i) d = radd(d, f[i]);
     d = inject_on(p, g, a, inj, n.y, d);
+    dn = d;
     const uint32_t pc = (uint32_t)psi_index(g, n.x, n.y, n.z);
     const int sy = g.pxg, sz = (g.ly + 2) * g.pxg;
     pr.ready();
     collide<float>(
         p, d, pr.self(pc),
-        [&](int i) { return pr.nb(pc + (ex(i) + ey(i) * sy + ez(i) * sz), i); },
+        [&](int i) {
+          const float v = pr.nb(pc + (ex(i) + ey(i) * sy + ez(i) * sz), i);
+          if (STATS) low |= (v < low_T ? 1u : 0u) << opp(i);
+          return v;
+        },
         f, ux, uy, uz);
   }
   if (WRITE_U) {
@@ -458,6 +472,7 @@ __device__ __forceinline__ void node_update0(T* cpop, uint32_t cs,
 #pragma unroll
   for (int e = 0; e < Q; ++e)
     PopPair<T>::st1(cpop + A[e], f[e], shift * weight<float>(e));
+  if (STATS) acc->add(p, dn, n.nb, low);
 }
 
 }  // namespace mlbm
