@@ -210,6 +210,12 @@ int32_t mlbm_get_step_kernel(const mlbm_lattice* lat);
  * 4 x 24. */
 mlbm_status mlbm_set_band_shape(mlbm_lattice* lat, int32_t rows,
                                 int32_t planes);
+/* COMPACT step schedule: 0 (default) launches the density pass and the
+ * update pass over the whole lattice; planes > 0 splits the step into
+ * chunks of that many z planes and runs density(chunk j + 1) before
+ * update(chunk j), so each chunk's update reads populations the density
+ * pass has just brought into L2.  Results are the same bits either way. */
+mlbm_status mlbm_set_chunk_planes(mlbm_lattice* lat, int32_t planes);
 /* Shape of the two-pass update kernel: tile rows (block = 32 x rows
  * threads, 1..8) and planes walked per block (1..1024).  Default 4 x 16. */
 mlbm_status mlbm_set_update_shape(mlbm_lattice* lat, int32_t rows,
@@ -332,8 +338,10 @@ mlbm_status mlbm_checkpoint_read(mlbm_lattice* lat, const char* path,
  * Its scratch is a fixed static device array (about 459 KB on every GPU that
  * loads the library, kept until exit), so nx may not exceed
  * MLBM_NOALLOC_MAX_LX (MLBM_ERR_ARG otherwise).  The first call on each
- * device looks up the array's device address; make it before any stream
- * capture starts, and make no call on a device after cudaDeviceReset (the
+ * device looks up the array's device address with cudaGetSymbolAddress,
+ * which may load the library's device code on that device; a caller that
+ * restricts which CUDA calls may run at a given point makes that first call
+ * during its setup.  Make no call on a device after cudaDeviceReset (the
  * kept address belongs to the reset context).  Calls share the array: calls
  * that overlap on the GPU race and must be serialised by the caller. */
 #define MLBM_NOALLOC_MAX_LX 4096

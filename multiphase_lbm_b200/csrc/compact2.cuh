@@ -135,16 +135,17 @@ __global__ void __launch_bounds__(kC2Threads, 5)
 }
 
 // With STATS the launch also gathers the phase statistics of the step's
-// density (stats_tap.cuh): every block writes its record into the
-// column-major partials `part` (ST_COUNT x gridDim.x), so no thread leaves
-// before the block's reduction.
+// density (stats_tap.cuh): block b writes its record as record bbase + b of
+// the column-major partials `part` (ST_COUNT x nblk; the step's update
+// launches fill consecutive record ranges), so no thread leaves before the
+// block's reduction.
 template <typename T, int PHASE, bool WRITE_U, bool STATS>
 __global__ void __launch_bounds__(kC2Threads, 3)
     k_cupdate(T* __restrict__ cpop, uint32_t cs, const uint2* __restrict__ cinfo,
               const uint2* __restrict__ wtab, int kbeg, int nfluid,
               const float* __restrict__ psi, float* __restrict__ vel, Geom g,
               Phys p, StepArgs a, bool inj, float low_T,
-              double* __restrict__ part) {
+              double* __restrict__ part, unsigned nblk, unsigned bbase) {
   const long long k = kbeg + c2_nodes_per_thread<PHASE>() *
                                  ((long long)blockIdx.x * kC2Threads + threadIdx.x);
   StatAcc acc;
@@ -159,7 +160,7 @@ __global__ void __launch_bounds__(kC2Threads, 3)
                                                   nfluid, PsiPlain{psi}, vel,
                                                   g, p, a, inj, low_T, &acc);
   }
-  if (STATS) stat_block_write<kC2Threads>(acc, part, gridDim.x);
+  if (STATS) stat_block_write<kC2Threads>(acc, part, nblk, bbase + blockIdx.x);
 }
 
 }  // namespace mlbm

@@ -24,8 +24,10 @@
 //
 // In host code the array's name is only a host-side stand-in, not a device
 // address.  The first call on each device therefore looks the real address
-// up with cudaGetSymbolAddress (with that device current) and keeps it; make
-// that first call on a device before any stream capture begins.  The kept
+// up with cudaGetSymbolAddress (with that device current) and keeps it; that
+// lookup may load the library's device code, so a caller that restricts
+// which CUDA calls may run at a given point makes the first call during its
+// setup.  The kept
 // address belongs to the device's primary context: a process that resets
 // the device (cudaDeviceReset) must not call this entry point afterwards.
 #include <cuda_runtime.h>

@@ -16,9 +16,10 @@
 // separate pass, io_kernels.cuh, runs).
 //
 // Counts and min/max are exact and independent of order; the FP64 sums are
-// folded in a fixed order (node, lane pair, warp tree, block, column), so the
-// result is deterministic, and equal to the separate pass's sums up to the
-// rounding of a different summation order.
+// folded in a fixed order (node, lane pair, warp tree, block, then the
+// block records by k_stats_final_cols), so the result is deterministic, and
+// equal to the separate pass's sums up to the rounding of another
+// summation order.
 #pragma once
 
 #include <cstdint>
@@ -104,13 +105,13 @@ __device__ __forceinline__ float warp_max(float v) {
 }
 
 // Fold the block's accumulators (fixed order: warp trees, then warps
-// ascending) and write its record into column-major partials:
-// part[k * nblk + blockIdx.x] for statistic k.  Every thread of the block
-// must call it.
+// ascending) and write them as record `rec` of column-major partials:
+// part[k * nblk + rec] for statistic k.  Every thread of the block must
+// call it.
 template <int THREADS>
 __device__ __forceinline__ void stat_block_write(const StatAcc& a,
                                                  double* __restrict__ part,
-                                                 unsigned nblk) {
+                                                 unsigned nblk, unsigned rec) {
   constexpr int W = THREADS / 32;
   __shared__ double sh[ST_COUNT][W];
   double v[ST_COUNT];
@@ -139,7 +140,7 @@ __device__ __forceinline__ void stat_block_write(const StatAcc& a,
     double r = sh[k][0];
 #pragma unroll
     for (int w = 1; w < W; ++w) r = stat_op(k, r, sh[k][w]);
-    part[(size_t)k * nblk + blockIdx.x] = r;
+    part[(size_t)k * nblk + rec] = r;
   }
 }
 

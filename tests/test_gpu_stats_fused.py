@@ -85,7 +85,9 @@ def test_fused_statistics_match_the_separate_pass(storage, runs):
     shape = (64, 48, 40)
     fluid, rho = sphere_case(shape, seed=5 + storage, rmin=3.0, rmax=6.0,
                              porosity=0.55, rho0=1.0, amp=0.9)
-    got = _compare(capi, fluid, rho, storage, runs=runs, **DRAIN)
+    # spinodal bounds inside the density range, so every class is populated
+    kw = dict(DRAIN, rhol_spinodal=0.45, rhog_spinodal=0.3)
+    got = _compare(capi, fluid, rho, storage, runs=runs, **kw)
     s = got[-1]
     # the case has liquid, vapour and both boundary kinds
     assert s["n_liquid"] > 0 and s["n_vapour"] > 0
