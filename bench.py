@@ -364,8 +364,6 @@ def measure(capi, torch, fluid, rho, storage_name, args, local, dist,
         lat.set_step_kernel(kernel_id)
     if args.band_shape:
         lat.set_band_shape(*[int(v) for v in args.band_shape.split(",")])
-    if args.chunk_planes is not None:
-        lat.set_chunk_planes(args.chunk_planes)
     kernel = lat.step_kernel
     lat.iterate(0, args.warmup)
     torch.cuda.synchronize()
@@ -395,8 +393,6 @@ def main():
                     choices=["auto", "band", "compact", "two-pass"])
     ap.add_argument("--band-shape", default=None,
                     help="rows,planes of the one-pass step's bands")
-    ap.add_argument("--chunk-planes", type=int, default=None,
-                    help="planes per chunk of the compact step (0: none)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 

@@ -210,12 +210,6 @@ int32_t mlbm_get_step_kernel(const mlbm_lattice* lat);
  * 4 x 24. */
 mlbm_status mlbm_set_band_shape(mlbm_lattice* lat, int32_t rows,
                                 int32_t planes);
-/* COMPACT step schedule: 0 (default) launches the density pass and the
- * update pass over the whole lattice; planes > 0 splits the step into
- * chunks of that many z planes and runs density(chunk j + 1) before
- * update(chunk j), so each chunk's update reads populations the density
- * pass has just brought into L2.  Results are the same bits either way. */
-mlbm_status mlbm_set_chunk_planes(mlbm_lattice* lat, int32_t planes);
 /* Shape of the two-pass update kernel: tile rows (block = 32 x rows
  * threads, 1..8) and planes walked per block (1..1024).  Default 4 x 16. */
 mlbm_status mlbm_set_update_shape(mlbm_lattice* lat, int32_t rows,

@@ -115,7 +115,6 @@ SIGNATURES = [
     ("mlbm_synchronize", C.c_int, [_VP]),
     ("mlbm_set_update_shape", C.c_int, [_VP, C.c_int32, C.c_int32]),
     ("mlbm_set_band_shape", C.c_int, [_VP, C.c_int32, C.c_int32]),
-    ("mlbm_set_chunk_planes", C.c_int, [_VP, C.c_int32]),
     ("mlbm_set_wait_limit", C.c_int, [_VP, C.c_uint64]),
     ("mlbm_test_stall_wait", C.c_int, [_VP]),
     ("mlbm_get_step_kernel", C.c_int32, [_VP]),
@@ -261,10 +260,6 @@ class Lattice:
     def test_stall_wait(self) -> None:
         """Make one wait of the next BAND launch run out (testing)."""
         check(lib().mlbm_test_stall_wait(self.h))
-
-    def set_chunk_planes(self, planes: int) -> None:
-        """COMPACT step in chunks of `planes` z planes (0: whole lattice)."""
-        check(lib().mlbm_set_chunk_planes(self.h, planes))
 
     def set_band_shape(self, rows: int = 4, planes: int = 24) -> None:
         """Tiling of KERNEL_BAND: rows per band (y) and planes per chunk (z)."""

@@ -916,13 +916,6 @@ mlbm_status mlbm_set_band_shape(mlbm_lattice* lat, int32_t rows,
   return compact_set_band_shape(lat, rows, planes);
 }
 
-mlbm_status mlbm_set_chunk_planes(mlbm_lattice* lat, int32_t planes) {
-  if (mlbm_status st = check_lat(lat)) return st;
-  if (planes < 0) return fail(MLBM_ERR_ARG, "negative chunk planes");
-  lat->compact.chunk_planes = planes;
-  return MLBM_OK;
-}
-
 mlbm_status mlbm_autotune(mlbm_lattice* lat, int64_t step0,
                           int32_t trial_steps, int32_t* out,
                           int32_t* steps_done) {

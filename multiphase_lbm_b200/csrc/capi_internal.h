@@ -30,9 +30,6 @@ struct CompactState {
   // one-pass step (band.cuh): the second population buffer and the tiling
   void* cpop_alt = nullptr;            // [Q][cs] populations (T)
   int band_rows = 4, band_planes = 24;  // requested rows per band, planes per chunk
-  // two-pass step: planes per chunk of the L2-blocked schedule (0: whole
-  // lattice per launch)
-  int chunk_planes = 0;
   // stage size (compact slots) of the shape last launched, and its key
   int band_slot = 0, band_slot_rows = -1, band_slot_nb = -1, band_slot_storage = -1;
 };

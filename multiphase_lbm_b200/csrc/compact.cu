@@ -323,98 +323,31 @@ void launch_c2_update_t(mlbm_lattice* lat, const StepArgs& a, bool wu, bool inj,
         lat->phys, a, inj, low_T, part, nblk, bbase);
 }
 
-// Compact ranges of the update launches of one step: the whole own range,
-// or (chunk_planes > 0, not a slab) runs of chunk_planes planes.
-struct Chunks {
-  std::vector<long long> kb, ke;
-};
-
-Chunks step_chunks(const mlbm_lattice* lat) {
-  const CompactState& c = lat->compact;
-  Chunks ch;
-  long long kb, ke;
-  own_range(lat, kb, ke);
-  const int lz = lat->g.lz, cp = c.chunk_planes;
-  if (lat->slab || cp <= 0 || cp >= lz) {
-    ch.kb.push_back(kb);
-    ch.ke.push_back(ke);
-    return ch;
-  }
-  for (int z0 = 0; z0 < lz; z0 += cp) {
-    ch.kb.push_back(c.plane_start[z0]);
-    ch.ke.push_back(c.plane_start[std::min(lz, z0 + cp)]);
-  }
-  return ch;
-}
-
-// One compact two-pass step.  Whole-lattice form: the density pass, then
-// the update pass.  Chunked form, so that the update pass finds a chunk's
-// populations still in L2 from the density pass: the density of the last
-// plane (the periodic neighbour of plane 0), then density(0), density(1),
-// update(0), density(2), update(1), ..., update(last) on even steps, and
-// the mirror order (plane 0 first, chunks downwards) on odd steps.  An update only
-// needs psi of its own and the two neighbouring planes, and every
-// population slot is read and written by one node's update only (AA), so a
-// chunk's update never touches slots the later density launches read.
-// With stats_out the update launches also gather the phase statistics of
-// the step (stats_tap.cuh) into one set of records, folded and copied with
-// the device error flag to stats_out (ST_COUNT + 1 doubles).
+// One compact two-pass step: the density pass, then the update pass.  With
+// stats_out the update pass also gathers the phase statistics of the step
+// (stats_tap.cuh), folded and copied with the device error flag to
+// stats_out (ST_COUNT + 1 doubles).
 template <typename T, int PHASE>
 mlbm_status two_pass_t(mlbm_lattice* lat, const StepArgs& a, bool wu, bool wr,
                        bool inj, double* stats_out) {
-  const CompactState& c = lat->compact;
-  const Chunks ch = step_chunks(lat);
-  const size_t n = ch.kb.size();
-  std::vector<unsigned> base(n + 1, 0u);
-  for (size_t j = 0; j < n; ++j)
-    base[j + 1] = base[j] + c2_grid(ch.kb[j], ch.ke[j], c2_nodes_per_thread<PHASE>());
-  const unsigned nblk = base[n];
-  double* part = nullptr;
-  if (stats_out) {
-    const size_t need = ((size_t)nblk + 1) * ST_COUNT * sizeof(double) + sizeof(double);
-    if (mlbm_status st = ensure_stats_scratch(lat, need)) return st;
-    part = lat->stats_scratch;
+  long long kb, ke;
+  own_range(lat, kb, ke);
+  launch_c2_density<T, PHASE>(lat, a, wr, inj, kb, ke);
+  if (!stats_out) {
+    launch_c2_update_t<T, PHASE, false>(lat, a, wu, inj, kb, ke, nullptr, 0u, 0u);
+    return MLBM_OK;
   }
-  auto update = [&](size_t j) {
-    if (stats_out)
-      launch_c2_update_t<T, PHASE, true>(lat, a, wu, inj, ch.kb[j], ch.ke[j],
-                                         part, nblk, base[j]);
-    else
-      launch_c2_update_t<T, PHASE, false>(lat, a, wu, inj, ch.kb[j], ch.ke[j],
-                                          nullptr, nblk, base[j]);
-  };
-  if (n == 1) {
-    launch_c2_density<T, PHASE>(lat, a, wr, inj, ch.kb[0], ch.ke[0]);
-    update(0);
-  } else if ((a.step & 1) == 0) {
-    const int lz = lat->g.lz;
-    launch_c2_density<T, PHASE>(lat, a, wr, inj, c.plane_start[lz - 1],
-                                c.plane_start[lz]);
-    for (size_t j = 0; j < n; ++j) {
-      launch_c2_density<T, PHASE>(lat, a, wr, inj, ch.kb[j], ch.ke[j]);
-      if (j > 0) update(j - 1);
-    }
-    update(n - 1);
-  } else {
-    // odd steps walk the chunks downwards, so a step starts on the chunks
-    // the previous step updated last (still in L2)
-    launch_c2_density<T, PHASE>(lat, a, wr, inj, c.plane_start[0],
-                                c.plane_start[1]);
-    for (size_t j = n; j-- > 0;) {
-      launch_c2_density<T, PHASE>(lat, a, wr, inj, ch.kb[j], ch.ke[j]);
-      if (j + 1 < n) update(j + 1);
-    }
-    update(0);
-  }
-  if (stats_out) {
-    double* fin = part + (size_t)nblk * ST_COUNT;
-    k_stats_final_cols<<<ST_COUNT, kStatColThreads, 0, lat->stream>>>(part, nblk,
-                                                                       lat->err, fin);
-    const cudaError_t e = cudaMemcpyAsync(stats_out, fin,
-                                          (ST_COUNT + 1) * sizeof(double),
-                                          cudaMemcpyDeviceToHost, lat->stream);
-    if (e != cudaSuccess) return cuda_fail(e, "statistics copy");
-  }
+  const unsigned nblk = c2_grid(kb, ke, c2_nodes_per_thread<PHASE>());
+  const size_t need = ((size_t)nblk + 1) * ST_COUNT * sizeof(double) + sizeof(double);
+  if (mlbm_status st = ensure_stats_scratch(lat, need)) return st;
+  double* part = lat->stats_scratch;
+  launch_c2_update_t<T, PHASE, true>(lat, a, wu, inj, kb, ke, part, nblk, 0u);
+  double* fin = part + (size_t)nblk * ST_COUNT;
+  k_stats_final_cols<<<ST_COUNT, kStatColThreads, 0, lat->stream>>>(part, nblk,
+                                                                     lat->err, fin);
+  const cudaError_t e = cudaMemcpyAsync(stats_out, fin, (ST_COUNT + 1) * sizeof(double),
+                                        cudaMemcpyDeviceToHost, lat->stream);
+  if (e != cudaSuccess) return cuda_fail(e, "statistics copy");
   return MLBM_OK;
 }
 

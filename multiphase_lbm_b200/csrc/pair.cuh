@@ -34,7 +34,6 @@
 #include "compact.cuh"
 #include "kernels.cuh"
 #include "lattice.cuh"
-#include "stats_tap.cuh"
 
 namespace mlbm {
 
@@ -319,9 +318,8 @@ __device__ __forceinline__ void pair_density(const T* cpop, uint32_t cs,
 }
 
 // Update pass of one pair (the work of k_cupdate for two nodes).  With
-// STATS, the pair's phase statistics are folded into *acc (stats_tap.cuh):
-// the neighbour psi the force loads, compared with low_T, give the
-// liquid-boundary test.
+// STATS, d_out receives the pair's densities and *n_out its node count, for
+// the phase statistics the kernel gathers after the update (stats_tap.cuh).
 template <typename T, int PHASE, bool WRITE_U, class PsiR, bool STATS = false>
 __device__ __forceinline__ void pair_update(T* cpop, uint32_t cs,
                                             const uint2* __restrict__ cinfo,
@@ -329,15 +327,14 @@ __device__ __forceinline__ void pair_update(T* cpop, uint32_t cs,
                                             int k, int nfluid, const PsiR& pr,
                                             float* vel, const Geom& g,
                                             const Phys& p, const StepArgs& a,
-                                            bool inj, float low_T = 0.f,
-                                            StatAcc* acc = nullptr) {
+                                            bool inj, float2* d_out = nullptr,
+                                            int* n_out = nullptr) {
   const Pair q = load_pair(cinfo, k, nfluid);
   uint32_t A[Q], B[Q];
   float2 f[Q];
   pair_load<T, PHASE>(cpop, cs, wtab, g, q, p.rho_shift, A, B, f);
   const float2 d = pair_rho(p, g, a, inj, q, f);
   float2 ux, uy, uz;
-  uint32_t lowa = 0u, lowb = 0u;  // bit i: psi of x - e_i below low_T
   {
     const uint32_t pa = (uint32_t)psi_index(g, q.a.x, q.a.y, q.a.z);
     const uint32_t pb = (uint32_t)psi_index(g, q.b.x, q.b.y, q.b.z);
@@ -347,12 +344,7 @@ __device__ __forceinline__ void pair_update(T* cpop, uint32_t cs,
         p, d, make_float2(pr.self(pa), pr.self(pb)),
         [&](int i) {
           const int o = ex(i) + ey(i) * sy + ez(i) * sz;
-          const float va = pr.nb(pa + o, i), vb = pr.nb(pb + o, i);
-          if (STATS) {  // x + e_i is x - e_opp(i)
-            lowa |= (va < low_T ? 1u : 0u) << opp(i);
-            lowb |= (vb < low_T ? 1u : 0u) << opp(i);
-          }
-          return make_float2(va, vb);
+          return make_float2(pr.nb(pa + o, i), pr.nb(pb + o, i));
         },
         f, ux, uy, uz);
   }
@@ -378,8 +370,8 @@ __device__ __forceinline__ void pair_update(T* cpop, uint32_t cs,
   }
   pair_scatter<T, PHASE>(cpop, cs, k, A, B, p.rho_shift, f);
   if (STATS) {
-    acc->add(p, d.x, q.a.nb, lowa);
-    if (q.two) acc->add(p, d.y, q.b.nb, lowb);
+    *d_out = d;
+    *n_out = q.two ? 2 : 1;
   }
 }
 
@@ -425,8 +417,8 @@ __device__ __forceinline__ void node_update0(T* cpop, uint32_t cs,
                                              int k, const PsiR& pr, float* vel,
                                              const Geom& g, const Phys& p,
                                              const StepArgs& a, bool inj,
-                                             float low_T = 0.f,
-                                             StatAcc* acc = nullptr) {
+                                             float2* d_out = nullptr,
+                                             int* n_out = nullptr) {
   const PairNode n = pair_node(cinfo, k);
   if (!(n.nb & NB_SELF)) return;
   const float shift = p.rho_shift;
@@ -434,14 +426,10 @@ __device__ __forceinline__ void node_update0(T* cpop, uint32_t cs,
   aa_addresses0(wtab, g, cs, n, A);
   float f[Q];
   float ux = 0.f, uy = 0.f, uz = 0.f;
-  float dn;          // the node's density (statistics)
-  uint32_t low = 0u;  // bit i: psi of x - e_i below low_T
+  float dn;  // the node's density (statistics)
   if (n.kind) {
     dn = slab_density(p, n.kind);
     slab_populations<float>(dn, f);
-    // a slab node loads no neighbour psi: the liquid test reads them here
-    if (STATS && dn > p.rhol_spinodal)
-      low = stat_low_bits(pr.psi, g, n.x, n.y, n.z, low_T);
   } else {
 #pragma unroll
     for (int e = 0; e < Q; ++e)
@@ -456,11 +444,7 @@ __device__ __forceinline__ void node_update0(T* cpop, uint32_t cs,
     pr.ready();
     collide<float>(
         p, d, pr.self(pc),
-        [&](int i) {
-          const float v = pr.nb(pc + (ex(i) + ey(i) * sy + ez(i) * sz), i);
-          if (STATS) low |= (v < low_T ? 1u : 0u) << opp(i);
-          return v;
-        },
+        [&](int i) { return pr.nb(pc + (ex(i) + ey(i) * sy + ez(i) * sz), i); },
         f, ux, uy, uz);
   }
   if (WRITE_U) {
@@ -472,7 +456,10 @@ __device__ __forceinline__ void node_update0(T* cpop, uint32_t cs,
 #pragma unroll
   for (int e = 0; e < Q; ++e)
     PopPair<T>::st1(cpop + A[e], f[e], shift * weight<float>(e));
-  if (STATS) acc->add(p, dn, n.nb, low);
+  if (STATS) {
+    d_out->x = dn;
+    *n_out = 1;
+  }
 }
 
 }  // namespace mlbm

@@ -6,9 +6,10 @@
 // density and pressure and, for a liquid node (rho > rhol), the first of its
 // 18 neighbours x - e_i (i = 1..18 in order) that is solid or not liquid
 // (rho < rhol).  The update pass already forms the node's density (the same
-// sum, in the same order, that the density pass stored) and loads psi of all
-// 18 neighbours for the interaction force, so the test "neighbour not liquid"
-// is read off the loaded psi as psi < T.  That equals rho < rhol for every
+// sum, in the same order, that the density pass stored) and has just loaded
+// psi of all 18 neighbours for the interaction force (so reading them again
+// after the update hits the cache), and the test "neighbour not liquid" is
+// read off psi as psi < T.  That equals rho < rhol for every
 // neighbour exactly when T separates psi(r) of all float densities r < rhol
 // from psi(r) of all others; k_psi_threshold checks that for the lattice's
 // psi function over all 2^32 float bit patterns and yields T, and the host
@@ -69,9 +70,8 @@ struct StatAcc {
   }
 };
 
-// The neighbour-psi test of one node read directly from the psi array (for
-// the drainage slab nodes, whose update writes fixed populations and loads no
-// neighbour psi).  psi_index layout; periodic images live in the halo.
+// The neighbour-psi test of one node: bit i set where psi of x - e_i is
+// below T (psi_index layout; periodic images live in the halo).
 __device__ __forceinline__ uint32_t stat_low_bits(const float* __restrict__ psi,
                                                   const Geom& g, int x, int y,
                                                   int z, float T) {
@@ -84,6 +84,20 @@ __device__ __forceinline__ uint32_t stat_low_bits(const float* __restrict__ psi,
     low |= (v < T ? 1u : 0u) << i;
   }
   return low;
+}
+
+// Fold one fluid node whose update is done: its node-table entry
+// (neighbour word, packed x, y, z) and density r; a liquid node reads the
+// psi of its 18 neighbours for the boundary test.
+__device__ __forceinline__ void stat_fold_node(StatAcc& acc, const Phys& p,
+                                               const Geom& g,
+                                               const float* __restrict__ psi,
+                                               uint2 ci, float r, float T) {
+  uint32_t low = 0u;
+  if (r > p.rhol_spinodal)
+    low = stat_low_bits(psi, g, (int)(ci.y & 2047u), (int)((ci.y >> 11) & 2047u),
+                        (int)(ci.y >> 22), T);
+  acc.add(p, r, ci.x, low);
 }
 
 __device__ __forceinline__ double warp_sum(double v) {

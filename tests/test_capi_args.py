@@ -102,4 +102,3 @@ def test_fused_statistics_entry_points_refuse_bad_arguments():
     t = C.c_float()
     e = C.c_int32()
     _refused(L.mlbm_stats_threshold(None, C.byref(t), C.byref(e)), "null lattice")
-    _refused(L.mlbm_set_chunk_planes(None, 4), "null lattice")

@@ -78,53 +78,6 @@ def test_compact_two_pass_bit_identical(shape, storage):
         assert np.array_equal(u, v)
 
 
-@pytest.mark.parametrize("storage", [0, 1])
-@pytest.mark.parametrize("shape", [(40, 32, 24), (33, 5, 7), (24, 20, 1),
-                                   (17, 2, 9)])
-def test_chunked_schedule_bit_identical(shape, storage):
-    """The L2-blocked schedule (density of chunk j + 1 before the update of
-    chunk j) gives the bits of the whole-lattice schedule, for chunks of one
-    plane, of a few planes (the last one short), of all planes but one and
-    of all planes; with the statistics gathered by the update pass too."""
-    import torch
-
-    from multiphase_lbm_b200 import capi
-    fluid, rho = sphere_case(shape, seed=sum(shape) + 7 * storage, rmin=1.5,
-                             rmax=3.5, porosity=0.6, rho0=1.0, amp=0.8)
-    kw = dict(G=-5.0, rhos=0.223144, tau=1.0, rho_shift=1.0,
-              rho_inject_period=4, rho_increment=0.002, inject_position=0.3)
-    if shape[0] >= 8:
-        kw.update(inlet_width=2, outlet_width=1, rho_inlet=0.17, rho_outlet=1.9)
-    raw = torch.zeros(capi.STATS_RAW_LEN, dtype=torch.float64).pin_memory().numpy()
-
-    def run(chunk):
-        lat = _lattice(capi, shape, fluid, rho, capi.KERNEL_COMPACT,
-                       storage=storage, **kw)
-        lat.set_chunk_planes(chunk)
-        lat.iterate(0, 13)
-        lat.iterate_stats_async(13, 2, raw)
-        lat.synchronize()
-        st = lat.stats_from_raw(raw).copy()
-        lat.iterate(15, 1, write_velocity=True)
-        out = (lat.field("rho"), lat.field("f"), lat.field("velocity"),
-               lat.field("psi"))
-        lat.close()
-        return out, st
-
-    want, st0 = run(0)
-    lz = shape[2]
-    for chunk in sorted({1, 3, max(1, lz - 1), lz}):
-        got, st = run(chunk)
-        for u, v in zip(got, want):
-            assert np.array_equal(u, v), chunk
-        # counts and extremes exact; sums up to the summation order
-        for k, v in st0.items():
-            if k.startswith("n_") or k.startswith(("min_", "max_")):
-                assert st[k] == v, (chunk, k)
-            else:
-                assert abs(st[k] - v) <= 1e-12 * max(abs(v), 1e-300), (chunk, k)
-
-
 def test_kernel_switching_keeps_the_state():
     """band -> two-pass -> compact -> band -> two-pass, against two-pass
     throughout: the state moves between the layouts and buffers exactly."""
