@@ -496,10 +496,9 @@ def main():
 def run_e2e(capi, torch, fluid, rho, params, storage, device, steps, dist,
             kernel_id=None):
     """MLUPS through the public C ABI with host buffers (pinned).  Every
-    step's phase statistics are read back: gathered by the step's own update
-    pass and copied without waiting (mlbm_iterate_stats_async), and read on
-    the host one step later, while the next step runs, so the GPU does not
-    idle on the host's read."""
+    step's phase statistics are read back: enqueued without waiting
+    (mlbm_phase_stats_async) and read on the host one step later, while the
+    next step runs, so the GPU does not idle on the host's read."""
     fl_h = torch.from_numpy(fluid).pin_memory().numpy()
     rho_h = torch.from_numpy(rho).pin_memory().numpy()
     out_h = torch.empty(fluid.shape, dtype=torch.float32).pin_memory().numpy()
@@ -525,11 +524,9 @@ def run_e2e(capi, torch, fluid, rho, params, storage, device, steps, dist,
     lat.initialize()
     mark()
     sat = []
-    lat.stats_threshold()  # the one-time check behind the fused statistics
-    mark()
     for k in range(steps):
-        # the step, and a device->host read of its statistics
-        lat.iterate_stats_async(k, 1, raw[k % 2])
+        lat.iterate(k, 1)
+        lat.stats_async(raw[k % 2])  # device->host read of the step's stats
         done[k % 2].record()
         if k == 0:
             mark()  # the first step builds the fluid-only tables
@@ -544,8 +541,7 @@ def run_e2e(capi, torch, fluid, rho, params, storage, device, steps, dist,
                                     out_h.ctypes.data))
     dt = time.perf_counter() - t0
     edges = [t0] + marks + [t0 + dt]
-    parts = ["upload", "initialize", "stats_threshold", "first_step",
-             "steps_after_first",
+    parts = ["upload", "initialize", "first_step", "steps_after_first",
              "download"]
     breakdown = {k: round((b - a) * 1e3, 3)
                  for k, a, b in zip(parts, edges[:-1], edges[1:])}

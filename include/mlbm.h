@@ -261,26 +261,6 @@ mlbm_status mlbm_phase_stats(mlbm_lattice* lat, mlbm_stats* out);
 mlbm_status mlbm_phase_stats_async(mlbm_lattice* lat, double* raw);
 mlbm_status mlbm_stats_from_raw(mlbm_lattice* lat, const double* raw,
                                 mlbm_stats* out);
-/* mlbm_iterate followed by mlbm_phase_stats_async, with the statistics of
- * the last step gathered by that step's own update pass where it can (the
- * compact step kernels, FP32/FP16 storage, and a psi function for which
- * psi < T decides rho < rhol exactly: checked once per parameter set over
- * every float density, which takes a few milliseconds and synchronises
- * the stream); otherwise the separate statistics pass runs after the
- * steps.  The counts, minima and maxima equal mlbm_phase_stats's; the sums
- * equal them up to the rounding of another summation order.  The
- * reference's driver (calc_cluster after multiphaselbm_iteration on a
- * statPeriod step, src/multiphase_lbm.cu:592-597) needs both calls; this
- * is one pass fewer over the lattice.  nsteps >= 1; `raw` as for
- * mlbm_phase_stats_async. */
-mlbm_status mlbm_iterate_stats_async(mlbm_lattice* lat, int64_t step0,
-                                     int32_t nsteps, int32_t reverse,
-                                     uint32_t inject_type, uint32_t flags,
-                                     double* raw);
-/* The threshold behind it for the lattice's parameters: *exact = 1 when
- * psi < *T equals rho < rhol_spinodal for every float density (then the
- * update pass gathers the statistics), else 0.  Synchronises the stream. */
-mlbm_status mlbm_stats_threshold(mlbm_lattice* lat, float* T, int32_t* exact);
 /* Per-x-plane counts of fluid and liquid nodes (int64[nx] each).  Sync. */
 mlbm_status mlbm_plane_profile(mlbm_lattice* lat, int64_t* n_fluid_x,
                                int64_t* n_liquid_x);

@@ -126,10 +126,6 @@ SIGNATURES = [
                                      _VP]),
     ("mlbm_phase_stats_async", C.c_int, [_VP, _VP]),
     ("mlbm_stats_from_raw", C.c_int, [_VP, _VP, C.POINTER(Stats)]),
-    ("mlbm_iterate_stats_async", C.c_int, [_VP, C.c_int64, C.c_int32, C.c_int32,
-                                           C.c_uint32, C.c_uint32, _VP]),
-    ("mlbm_stats_threshold", C.c_int, [_VP, C.POINTER(C.c_float),
-                                       C.POINTER(C.c_int32)]),
     ("mlbm_slab_ring_create", C.c_int, [_VP, C.c_int32, C.POINTER(_VP)]),
     ("mlbm_slab_ring_exchange", C.c_int, [_VP, C.c_int32]),
     ("mlbm_slab_ring_destroy", C.c_int, [_VP]),
@@ -349,24 +345,6 @@ class Lattice:
         if raw.dtype != np.float64 or raw.size < STATS_RAW_LEN:
             raise ValueError(f"raw must be float64[{STATS_RAW_LEN}]")
         check(lib().mlbm_phase_stats_async(self.h, _ptr(raw)))
-
-    def iterate_stats_async(self, step0: int, nsteps: int, raw: np.ndarray,
-                            reverse: int = 1, inject_type: int = 0,
-                            write_velocity: bool = False) -> None:
-        """iterate() and then stats_async() of the last step, gathered by
-        that step's update pass where the kernels allow it."""
-        if raw.dtype != np.float64 or raw.size < STATS_RAW_LEN:
-            raise ValueError(f"raw must be float64[{STATS_RAW_LEN}]")
-        check(lib().mlbm_iterate_stats_async(
-            self.h, step0, nsteps, reverse, inject_type,
-            ITER_WRITE_VELOCITY if write_velocity else 0, _ptr(raw)))
-
-    def stats_threshold(self) -> tuple:
-        """(T, exact): psi < T decides rho < rhol exactly when exact."""
-        t = C.c_float()
-        e = C.c_int32()
-        check(lib().mlbm_stats_threshold(self.h, C.byref(t), C.byref(e)))
-        return t.value, bool(e.value)
 
     def stats_from_raw(self, raw: np.ndarray) -> dict:
         s = Stats()

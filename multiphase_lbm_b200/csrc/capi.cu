@@ -214,8 +214,7 @@ int effective_kernel(const mlbm_lattice* lat) {
 template <typename T>
 mlbm_status launch_steps(mlbm_lattice* lat, int64_t step0, int32_t nsteps,
                          int32_t reverse, uint32_t inject_type,
-                         uint32_t flags, double* stats_out = nullptr,
-                         bool* stats_done = nullptr) {
+                         uint32_t flags) {
   const int kind = effective_kernel(lat);
   bool compact = false, band = false;
   if constexpr (!std::is_same<T, double>::value) {
@@ -247,16 +246,9 @@ mlbm_status launch_steps(mlbm_lattice* lat, int64_t step0, int32_t nsteps,
     // two-pass step gets there
     const bool one_pass = band && lat->phase == 1;
     if constexpr (!std::is_same<T, double>::value) {
-      if (one_pass) {
-        st = launch_compact_band<T>(lat, a, wu, last);
-      } else if (compact) {
-        // the last step's update pass gathers the statistics when asked
-        double* so = last ? stats_out : nullptr;
-        st = launch_compact_two_pass<T>(lat, a, wu, last, so);
-        if (so && !st && stats_done) *stats_done = true;
-      } else {
-        st = launch_two_pass<T>(lat, a, wu, last);
-      }
+      if (one_pass) st = launch_compact_band<T>(lat, a, wu, last);
+      else if (compact) st = launch_compact_two_pass<T>(lat, a, wu, last);
+      else st = launch_two_pass<T>(lat, a, wu, last);
     } else {
       st = launch_two_pass<T>(lat, a, wu, last);
     }
@@ -657,20 +649,6 @@ mlbm_status mlbm_download_field(mlbm_lattice* lat, int32_t field,
 
 }  // extern "C"
 
-namespace mlbm {
-mlbm_status ensure_stats_scratch(mlbm_lattice* lat, size_t need) {
-  if (lat->stats_scratch_bytes >= need) return MLBM_OK;
-  // a larger area: earlier calls may still be reading the old one
-  CUDA_TRY(cudaStreamSynchronize(lat->stream), "stats");
-  cudaFree(lat->stats_scratch);
-  lat->stats_scratch = nullptr;
-  lat->stats_scratch_bytes = 0;
-  CUDA_TRY(cudaMalloc((void**)&lat->stats_scratch, need), "stats scratch");
-  lat->stats_scratch_bytes = need;
-  return MLBM_OK;
-}
-}  // namespace mlbm
-
 namespace {
 
 // Enqueue the phase statistics reduction and the copy of its ST_COUNT + 1
@@ -695,7 +673,15 @@ mlbm_status stats_enqueue(mlbm_lattice* lat, double* h) {
                                 ? (c.nfluid + kStatSlots - 1) / kStatSlots
                                 : (long long)grid.x * grid.y * grid.z;
   const size_t need = ((size_t)nblocks + 1) * ST_COUNT * sizeof(double) + sizeof(double);
-  if (mlbm_status st = ensure_stats_scratch(lat, need)) return st;
+  if (lat->stats_scratch_bytes < need) {
+    // a larger area: earlier calls may still be reading the old one
+    CUDA_TRY(cudaStreamSynchronize(lat->stream), "stats");
+    cudaFree(lat->stats_scratch);
+    lat->stats_scratch = nullptr;
+    lat->stats_scratch_bytes = 0;
+    CUDA_TRY(cudaMalloc((void**)&lat->stats_scratch, need), "stats scratch");
+    lat->stats_scratch_bytes = need;
+  }
   double* partial = lat->stats_scratch;
   double* fin = partial + (size_t)nblocks * ST_COUNT;
   if (fluid_list) {
@@ -769,59 +755,6 @@ mlbm_status mlbm_phase_stats(mlbm_lattice* lat, mlbm_stats* out) {
 
 mlbm_status mlbm_phase_stats_async(mlbm_lattice* lat, double* raw) {
   return stats_enqueue(lat, raw);
-}
-
-mlbm_status mlbm_stats_threshold(mlbm_lattice* lat, float* T, int32_t* exact) {
-  if (mlbm_status st = check_lat(lat)) return st;
-  if (!T || !exact) return fail(MLBM_ERR_ARG, "null output");
-  if (!lat->has_params) return fail(MLBM_ERR_STATE, "threshold before params");
-  DeviceGuard restore_device;
-  if (mlbm_status st = activate(lat)) return st;
-  if (mlbm_status st = update_low_threshold(lat)) return st;
-  *T = lat->low.T;
-  *exact = lat->low.ok ? 1 : 0;
-  return MLBM_OK;
-}
-
-mlbm_status mlbm_iterate_stats_async(mlbm_lattice* lat, int64_t step0,
-                                     int32_t nsteps, int32_t reverse,
-                                     uint32_t inject_type, uint32_t flags,
-                                     double* raw) {
-  if (mlbm_status st = check_lat(lat)) return st;
-  if (!raw) return fail(MLBM_ERR_ARG, "null output");
-  if (nsteps < 1) return fail(MLBM_ERR_ARG, "iterate_stats needs at least one step");
-  if (!lat->initialized)
-    return fail(MLBM_ERR_STATE, "iterate before initialize");
-  if (lat->slab)
-    return fail(MLBM_ERR_STATE,
-                "iterate on a slab lattice: step it with mlbm_step_pass and "
-                "exchange its halos between the passes");
-  DeviceGuard restore_device;
-  if (mlbm_status st = activate(lat)) return st;
-  // the update pass gathers the statistics where psi < T is exactly
-  // rho < rhol (checked once per psi function)
-  double* fused = nullptr;
-  if (lat->storage != MLBM_STORE_F64) {
-    if (mlbm_status st = update_low_threshold(lat)) return st;
-    if (lat->low.ok) fused = raw;
-  }
-  bool done = false;
-  mlbm_status st;
-  switch (lat->storage) {
-    case MLBM_STORE_F32:
-      st = launch_steps<float>(lat, step0, nsteps, reverse, inject_type, flags,
-                               fused, &done);
-      break;
-    case MLBM_STORE_F16:
-      st = launch_steps<__half>(lat, step0, nsteps, reverse, inject_type, flags,
-                                fused, &done);
-      break;
-    default:
-      st = launch_steps<double>(lat, step0, nsteps, reverse, inject_type, flags);
-  }
-  if (st) return st;
-  // the last step ran another kernel: the separate statistics pass
-  return done ? MLBM_OK : stats_enqueue(lat, raw);
 }
 
 mlbm_status mlbm_stats_from_raw(mlbm_lattice* lat, const double* raw,

@@ -34,16 +34,6 @@ struct CompactState {
   int band_slot = 0, band_slot_rows = -1, band_slot_nb = -1, band_slot_storage = -1;
 };
 
-// The psi threshold of the statistics gathered by the update pass
-// (stats_tap.cuh): ok when psi < T is exactly rho < rhol for every float
-// density, checked for the psi function of the parameters it was made for.
-struct LowThreshold {
-  bool valid = false, ok = false;
-  int carn_star = 0;
-  float T_Tc = 0.f, G = 0.f, rhol = 0.f;
-  float T = 0.f;
-};
-
 // Bound of the step kernels' device waits, and the test switch that makes
 // one wait run out.
 constexpr unsigned long long kDefaultWaitNs = 1000000000ull;  // 1 s
@@ -69,7 +59,6 @@ struct mlbm_lattice {
   size_t staging_bytes = 0;
   double* stats_scratch = nullptr;
   size_t stats_scratch_bytes = 0;
-  mlbm::LowThreshold low{};     // statistics gathered by the update pass
 
   // update pass: z-march tiles and the TMA descriptor of the psi tensor
   mlbm::ZMarch zm{};
@@ -102,18 +91,9 @@ mlbm_status compact_leave(mlbm_lattice* lat);   // compact -> dense state
 mlbm_status compact_sync_dense(mlbm_lattice* lat);  // dense copy, stay compact
 void compact_invalidate(mlbm_lattice* lat);     // the mask changed
 void compact_free(mlbm_lattice* lat);
-// stats_out (host memory, ST_COUNT + 1 doubles, or null): the update pass
-// also gathers the step's phase statistics (only where lat->low.ok holds).
 template <typename T>
 mlbm_status launch_compact_two_pass(mlbm_lattice* lat, const StepArgs& a,
-                                    bool write_u, bool write_rho,
-                                    double* stats_out = nullptr);
-// Check (once per psi function) whether the update pass can gather the
-// phase statistics exactly: sets lat->low (synchronises the stream).
-mlbm_status update_low_threshold(mlbm_lattice* lat);
-// The statistics scratch area, grown to at least `bytes` (synchronises the
-// stream first when it grows: earlier calls may still read the old one).
-mlbm_status ensure_stats_scratch(mlbm_lattice* lat, size_t bytes);
+                                    bool write_u, bool write_rho);
 template <typename T>
 mlbm_status launch_compact_pass(mlbm_lattice* lat, const StepArgs& a, int pass,
                                 bool write_u, bool write_rho);

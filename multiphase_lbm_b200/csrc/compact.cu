@@ -5,7 +5,6 @@
 
 #include <algorithm>
 #include <cstdio>
-#include <cstring>
 #include <mutex>
 #include <vector>
 
@@ -228,127 +227,23 @@ void launch_c2_density(mlbm_lattice* lat, const StepArgs& a, bool wr, bool inj,
         a, inj);
 }
 
-// Fold the column-major partials: block k reduces statistic k over nblk
-// records (thread t folds records t, t + 512, ... ascending, from the
-// statistic's identity; then a fixed tree), and block 0 appends the device
-// error flag, as k_stats_final does.
-constexpr int kStatColThreads = 512;
-
-__global__ void __launch_bounds__(kStatColThreads)
-    k_stats_final_cols(const double* __restrict__ part, unsigned nblk,
-                       const int* __restrict__ err, double* __restrict__ out) {
-  __shared__ double sh[kStatColThreads];
-  const int k = blockIdx.x, tid = threadIdx.x;
-  const double* col = part + (size_t)k * nblk;
-  double v = stat_identity(k);
-  unsigned b = tid;
-#pragma unroll 1
-  for (; b + 3u * kStatColThreads < nblk; b += 4u * kStatColThreads) {
-    const double a0 = __ldg(col + b), a1 = __ldg(col + b + kStatColThreads),
-                 a2 = __ldg(col + b + 2u * kStatColThreads),
-                 a3 = __ldg(col + b + 3u * kStatColThreads);
-    v = stat_op(k, v, a0);
-    v = stat_op(k, v, a1);
-    v = stat_op(k, v, a2);
-    v = stat_op(k, v, a3);
-  }
-  for (; b < nblk; b += kStatColThreads) v = stat_op(k, v, __ldg(col + b));
-  sh[tid] = v;
-  __syncthreads();
-#pragma unroll 1
-  for (int s = kStatColThreads / 2; s > 0; s >>= 1) {
-    if (tid < s) sh[tid] = stat_op(k, sh[tid], sh[tid + s]);
-    __syncthreads();
-  }
-  if (tid == 0) {
-    out[k] = sh[0];
-    if (k == 0) out[ST_COUNT] = err ? (double)*err : 0.0;
-  }
-}
-
-// ---- the psi threshold -----------------------------------------------------
-// Order-preserving key of a float (larger float, larger key; -0 < +0).
-__device__ __forceinline__ unsigned float_key(float v) {
-  const unsigned b = __float_as_uint(v);
-  return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
-}
-
-// Over all 2^32 bit patterns r: out[0] = max key of psi(r) over r < rhol,
-// out[1] = min key of psi(r) over the other patterns whose psi is not NaN,
-// out[2] = 1 if some r < rhol has a NaN psi.  out must hold {0, ~0u, 0}.
-__global__ void __launch_bounds__(256)
-    k_psi_threshold(Phys p, unsigned* __restrict__ out) {
-  unsigned lo = 0u, hi = 0xffffffffu, bad = 0u;
-  const unsigned long long n = 1ull << 32;
-  const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
-  for (unsigned long long i = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
-       i < n; i += stride) {
-    const float r = __uint_as_float((unsigned)i);
-    const float s = psi_of<float>(p, r);
-    if (r < p.rhol_spinodal) {
-      if (s != s) bad = 1u;
-      else lo = max(lo, float_key(s));
-    } else if (s == s) {
-      hi = min(hi, float_key(s));
-    }
-  }
-  lo = __reduce_max_sync(0xffffffffu, lo);
-  hi = __reduce_min_sync(0xffffffffu, hi);
-  bad = __reduce_or_sync(0xffffffffu, bad);
-  if ((threadIdx.x & 31) == 0) {
-    atomicMax(out, lo);
-    atomicMin(out + 1, hi);
-    if (bad) atomicOr(out + 2, 1u);
-  }
-}
-
-template <typename T, int PHASE, bool STATS>
-void launch_c2_update_t(mlbm_lattice* lat, const StepArgs& a, bool wu, bool inj,
-                        long long kb, long long ke, double* part, unsigned nblk,
-                        unsigned bbase) {
+template <typename T, int PHASE>
+void launch_c2_update(mlbm_lattice* lat, const StepArgs& a, bool wu, bool inj,
+                      long long kb, long long ke) {
   const unsigned grid = c2_grid(kb, ke, c2_nodes_per_thread<PHASE>());
   if (grid == 0) return;
   const CompactState& c = lat->compact;
   T* cpop = static_cast<T*>(c.cpop);
   const uint32_t cs = (uint32_t)c.cs;
   const float* psi = static_cast<const float*>(lat->psi);
-  const float low_T = lat->low.T;
   if (wu)
-    k_cupdate<T, PHASE, true, STATS><<<grid, kC2Threads, 0, lat->stream>>>(
+    k_cupdate<T, PHASE, true><<<grid, kC2Threads, 0, lat->stream>>>(
         cpop, cs, c.cinfo, c.wtab, (int)kb, (int)ke, psi, lat->vel, lat->g,
-        lat->phys, a, inj, low_T, part, nblk, bbase);
+        lat->phys, a, inj);
   else
-    k_cupdate<T, PHASE, false, STATS><<<grid, kC2Threads, 0, lat->stream>>>(
+    k_cupdate<T, PHASE, false><<<grid, kC2Threads, 0, lat->stream>>>(
         cpop, cs, c.cinfo, c.wtab, (int)kb, (int)ke, psi, lat->vel, lat->g,
-        lat->phys, a, inj, low_T, part, nblk, bbase);
-}
-
-// One compact two-pass step: the density pass, then the update pass.  With
-// stats_out the update pass also gathers the phase statistics of the step
-// (stats_tap.cuh), folded and copied with the device error flag to
-// stats_out (ST_COUNT + 1 doubles).
-template <typename T, int PHASE>
-mlbm_status two_pass_t(mlbm_lattice* lat, const StepArgs& a, bool wu, bool wr,
-                       bool inj, double* stats_out) {
-  long long kb, ke;
-  own_range(lat, kb, ke);
-  launch_c2_density<T, PHASE>(lat, a, wr, inj, kb, ke);
-  if (!stats_out) {
-    launch_c2_update_t<T, PHASE, false>(lat, a, wu, inj, kb, ke, nullptr, 0u, 0u);
-    return MLBM_OK;
-  }
-  const unsigned nblk = c2_grid(kb, ke, c2_nodes_per_thread<PHASE>());
-  const size_t need = ((size_t)nblk + 1) * ST_COUNT * sizeof(double) + sizeof(double);
-  if (mlbm_status st = ensure_stats_scratch(lat, need)) return st;
-  double* part = lat->stats_scratch;
-  launch_c2_update_t<T, PHASE, true>(lat, a, wu, inj, kb, ke, part, nblk, 0u);
-  double* fin = part + (size_t)nblk * ST_COUNT;
-  k_stats_final_cols<<<ST_COUNT, kStatColThreads, 0, lat->stream>>>(part, nblk,
-                                                                     lat->err, fin);
-  const cudaError_t e = cudaMemcpyAsync(stats_out, fin, (ST_COUNT + 1) * sizeof(double),
-                                        cudaMemcpyDeviceToHost, lat->stream);
-  if (e != cudaSuccess) return cuda_fail(e, "statistics copy");
-  return MLBM_OK;
+        lat->phys, a, inj);
 }
 
 bool inject_now(const mlbm_lattice* lat, const StepArgs& a) {
@@ -360,59 +255,24 @@ bool inject_now(const mlbm_lattice* lat, const StepArgs& a) {
 
 template <typename T>
 mlbm_status launch_compact_two_pass(mlbm_lattice* lat, const StepArgs& a,
-                                    bool write_u, bool write_rho,
-                                    double* stats_out) {
+                                    bool write_u, bool write_rho) {
   const bool inj = inject_now(lat, a);
-  const mlbm_status st =
-      lat->phase == 0 ? two_pass_t<T, 0>(lat, a, write_u, write_rho, inj, stats_out)
-                      : two_pass_t<T, 1>(lat, a, write_u, write_rho, inj, stats_out);
-  if (st) return st;
+  long long kb, ke;
+  own_range(lat, kb, ke);
+  if (lat->phase == 0) {
+    launch_c2_density<T, 0>(lat, a, write_rho, inj, kb, ke);
+    launch_c2_update<T, 0>(lat, a, write_u, inj, kb, ke);
+  } else {
+    launch_c2_density<T, 1>(lat, a, write_rho, inj, kb, ke);
+    launch_c2_update<T, 1>(lat, a, write_u, inj, kb, ke);
+  }
   const cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(e, "compact two-pass launch");
   return MLBM_OK;
 }
 
-template mlbm_status launch_compact_two_pass<float>(mlbm_lattice*, const StepArgs&,
-                                                    bool, bool, double*);
-template mlbm_status launch_compact_two_pass<__half>(mlbm_lattice*, const StepArgs&,
-                                                     bool, bool, double*);
-
-mlbm_status update_low_threshold(mlbm_lattice* lat) {
-  const Phys& p = lat->phys;
-  LowThreshold& t = lat->low;
-  if (t.valid && t.carn_star == p.carn_star && t.T_Tc == p.T_Tc && t.G == p.G &&
-      t.rhol == p.rhol_spinodal)
-    return MLBM_OK;
-  const unsigned init[3] = {0u, 0xffffffffu, 0u};
-  unsigned got[3];
-  if (mlbm_status st = ensure_stats_scratch(lat, 64)) return st;
-  unsigned* dev = reinterpret_cast<unsigned*>(lat->stats_scratch);
-  cudaError_t e = cudaMemcpyAsync(dev, init, sizeof init, cudaMemcpyHostToDevice,
-                                  lat->stream);
-  if (e == cudaSuccess) {
-    k_psi_threshold<<<8 * 148, 256, 0, lat->stream>>>(p, dev);
-    e = cudaGetLastError();
-  }
-  if (e == cudaSuccess)
-    e = cudaMemcpyAsync(got, dev, sizeof got, cudaMemcpyDeviceToHost, lat->stream);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(lat->stream);
-  if (e != cudaSuccess) return cuda_fail(e, "psi threshold");
-  auto from_key = [](unsigned k) {
-    const unsigned b = (k & 0x80000000u) ? (k & 0x7fffffffu) : ~k;
-    float v;
-    std::memcpy(&v, &b, sizeof v);
-    return v;
-  };
-  t.valid = true;
-  t.carn_star = p.carn_star;
-  t.T_Tc = p.T_Tc;
-  t.G = p.G;
-  t.rhol = p.rhol_spinodal;
-  t.T = from_key(got[1]);
-  // every density below rhol must give psi < T, as floats (-0 == +0)
-  t.ok = got[2] == 0u && got[1] != 0xffffffffu && from_key(got[0]) < t.T;
-  return MLBM_OK;
-}
+template mlbm_status launch_compact_two_pass<float>(mlbm_lattice*, const StepArgs&, bool, bool);
+template mlbm_status launch_compact_two_pass<__half>(mlbm_lattice*, const StepArgs&, bool, bool);
 
 // One pass of the compact two-pass step (0: density, 1: update) in the
 // lattice's current AA phase; the caller flips the phase after the update.
@@ -428,10 +288,8 @@ mlbm_status launch_compact_pass(mlbm_lattice* lat, const StepArgs& a, int pass,
   } else {
     long long kb, ke;
     own_range(lat, kb, ke);
-    if (lat->phase == 0)
-      launch_c2_update_t<T, 0, false>(lat, a, write_u, inj, kb, ke, nullptr, 0u, 0u);
-    else
-      launch_c2_update_t<T, 1, false>(lat, a, write_u, inj, kb, ke, nullptr, 0u, 0u);
+    if (lat->phase == 0) launch_c2_update<T, 0>(lat, a, write_u, inj, kb, ke);
+    else launch_c2_update<T, 1>(lat, a, write_u, inj, kb, ke);
   }
   const cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(e, "compact pass launch");

@@ -103,7 +103,6 @@ static __global__ void k_wtab(const uint32_t* __restrict__ mask,
 }  // namespace mlbm
 
 #include "pair.cuh"
-#include "stats_tap.cuh"
 
 namespace mlbm {
 
@@ -135,40 +134,21 @@ __global__ void __launch_bounds__(kC2Threads, 5)
                                   rho_out, psi, g, p, a, inj);
 }
 
-// With STATS the launch also gathers the phase statistics of the step's
-// density (stats_tap.cuh) once the update of its nodes is done: only the
-// densities stay live across the update; node words and the neighbour psi
-// of the liquid test are read again (cache hits).  Block b writes its
-// record as record bbase + b of the column-major partials `part`
-// (ST_COUNT x nblk), so no thread leaves before the block's reduction.
-template <typename T, int PHASE, bool WRITE_U, bool STATS>
+template <typename T, int PHASE, bool WRITE_U>
 __global__ void __launch_bounds__(kC2Threads, 3)
     k_cupdate(T* __restrict__ cpop, uint32_t cs, const uint2* __restrict__ cinfo,
               const uint2* __restrict__ wtab, int kbeg, int nfluid,
               const float* __restrict__ psi, float* __restrict__ vel, Geom g,
-              Phys p, StepArgs a, bool inj, float low_T,
-              double* __restrict__ part, unsigned nblk, unsigned bbase) {
+              Phys p, StepArgs a, bool inj) {
   const long long k = kbeg + c2_nodes_per_thread<PHASE>() *
                                  ((long long)blockIdx.x * kC2Threads + threadIdx.x);
-  float2 d = make_float2(0.f, 0.f);
-  int n = 0;  // nodes updated by this thread (statistics)
-  if (k < nfluid) {
-    if (PHASE == 0)
-      node_update0<T, WRITE_U, PsiPlain, STATS>(cpop, cs, cinfo, wtab, (int)k,
-                                                PsiPlain{psi}, vel, g, p, a,
-                                                inj, &d, &n);
-    else
-      pair_update<T, 1, WRITE_U, PsiPlain, STATS>(cpop, cs, cinfo, wtab, (int)k,
-                                                  nfluid, PsiPlain{psi}, vel,
-                                                  g, p, a, inj, &d, &n);
-  }
-  if (STATS) {
-    StatAcc acc;
-    acc.clear();
-    if (n > 0) stat_fold_node(acc, p, g, psi, __ldg(cinfo + k), d.x, low_T);
-    if (n > 1) stat_fold_node(acc, p, g, psi, __ldg(cinfo + k + 1), d.y, low_T);
-    stat_block_write<kC2Threads>(acc, part, nblk, bbase + (unsigned)blockIdx.x);
-  }
+  if (k >= nfluid) return;
+  if (PHASE == 0)
+    node_update0<T, WRITE_U>(cpop, cs, cinfo, wtab, (int)k, PsiPlain{psi}, vel,
+                             g, p, a, inj);
+  else
+    pair_update<T, 1, WRITE_U>(cpop, cs, cinfo, wtab, (int)k, nfluid,
+                               PsiPlain{psi}, vel, g, p, a, inj);
 }
 
 }  // namespace mlbm

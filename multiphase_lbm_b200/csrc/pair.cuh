@@ -317,18 +317,15 @@ __device__ __forceinline__ void pair_density(const T* cpop, uint32_t cs,
   if (q.two) store_psi<float>(psi, g, q.b.x, q.b.y, q.b.z, psi_of<float>(p, d.y));
 }
 
-// Update pass of one pair (the work of k_cupdate for two nodes).  With
-// STATS, d_out receives the pair's densities and *n_out its node count, for
-// the phase statistics the kernel gathers after the update (stats_tap.cuh).
-template <typename T, int PHASE, bool WRITE_U, class PsiR, bool STATS = false>
+// Update pass of one pair (the work of k_cupdate for two nodes).
+template <typename T, int PHASE, bool WRITE_U, class PsiR>
 __device__ __forceinline__ void pair_update(T* cpop, uint32_t cs,
                                             const uint2* __restrict__ cinfo,
                                             const uint2* __restrict__ wtab,
                                             int k, int nfluid, const PsiR& pr,
                                             float* vel, const Geom& g,
                                             const Phys& p, const StepArgs& a,
-                                            bool inj, float2* d_out = nullptr,
-                                            int* n_out = nullptr) {
+                                            bool inj) {
   const Pair q = load_pair(cinfo, k, nfluid);
   uint32_t A[Q], B[Q];
   float2 f[Q];
@@ -369,10 +366,6 @@ __device__ __forceinline__ void pair_update(T* cpop, uint32_t cs,
     vel[3 * nb + 2] = uz.y;
   }
   pair_scatter<T, PHASE>(cpop, cs, k, A, B, p.rho_shift, f);
-  if (STATS) {
-    *d_out = d;
-    *n_out = q.two ? 2 : 1;
-  }
 }
 
 
@@ -410,15 +403,13 @@ __device__ __forceinline__ void node_density0(const T* cpop, uint32_t cs,
   store_psi<float>(psi, g, n.x, n.y, n.z, psi_of<float>(p, d));
 }
 
-template <typename T, bool WRITE_U, class PsiR, bool STATS = false>
+template <typename T, bool WRITE_U, class PsiR>
 __device__ __forceinline__ void node_update0(T* cpop, uint32_t cs,
                                              const uint2* __restrict__ cinfo,
                                              const uint2* __restrict__ wtab,
                                              int k, const PsiR& pr, float* vel,
                                              const Geom& g, const Phys& p,
-                                             const StepArgs& a, bool inj,
-                                             float2* d_out = nullptr,
-                                             int* n_out = nullptr) {
+                                             const StepArgs& a, bool inj) {
   const PairNode n = pair_node(cinfo, k);
   if (!(n.nb & NB_SELF)) return;
   const float shift = p.rho_shift;
@@ -426,10 +417,8 @@ __device__ __forceinline__ void node_update0(T* cpop, uint32_t cs,
   aa_addresses0(wtab, g, cs, n, A);
   float f[Q];
   float ux = 0.f, uy = 0.f, uz = 0.f;
-  float dn;  // the node's density (statistics)
   if (n.kind) {
-    dn = slab_density(p, n.kind);
-    slab_populations<float>(dn, f);
+    slab_populations<float>(slab_density(p, n.kind), f);
   } else {
 #pragma unroll
     for (int e = 0; e < Q; ++e)
@@ -438,7 +427,6 @@ __device__ __forceinline__ void node_update0(T* cpop, uint32_t cs,
 #pragma unroll
     for (int i = 0; i < Q; ++i) d = radd(d, f[i]);
     d = inject_on(p, g, a, inj, n.y, d);
-    dn = d;
     const uint32_t pc = (uint32_t)psi_index(g, n.x, n.y, n.z);
     const int sy = g.pxg, sz = (g.ly + 2) * g.pxg;
     pr.ready();
@@ -456,10 +444,6 @@ __device__ __forceinline__ void node_update0(T* cpop, uint32_t cs,
 #pragma unroll
   for (int e = 0; e < Q; ++e)
     PopPair<T>::st1(cpop + A[e], f[e], shift * weight<float>(e));
-  if (STATS) {
-    d_out->x = dn;
-    *n_out = 1;
-  }
 }
 
 }  // namespace mlbm

@@ -93,12 +93,3 @@ def test_checkpoint_entry_points_refuse_bad_arguments():
     _refused(L.mlbm_checkpoint_info(img.ctypes.data, img.nbytes, None, None,
                                     None), "unsupported format version")
 
-
-def test_fused_statistics_entry_points_refuse_bad_arguments():
-    L = capi.lib()
-    raw = np.zeros(capi.STATS_RAW_LEN, np.float64)
-    _refused(L.mlbm_iterate_stats_async(None, 0, 1, 1, 0, 0, raw.ctypes.data),
-             "null lattice")
-    t = C.c_float()
-    e = C.c_int32()
-    _refused(L.mlbm_stats_threshold(None, C.byref(t), C.byref(e)), "null lattice")
