@@ -669,10 +669,13 @@ mlbm_status stats_enqueue(mlbm_lattice* lat, double* h) {
   const bool fluid_list = c.active && c.cinfo && lat->storage != MLBM_STORE_F64;
   const dim3 grid(lat->g.px / 32, (lat->g.ly + 7) / 8,
                   (lat->g.lz + kStatZ - 1) / kStatZ);
-  const long long nblocks = fluid_list
-                                ? (c.nfluid + kStatSlots - 1) / kStatSlots
-                                : (long long)grid.x * grid.y * grid.z;
-  const size_t need = ((size_t)nblocks + 1) * ST_COUNT * sizeof(double) + sizeof(double);
+  // (the fluid-list form launches one block at least: the last block to
+  // finish writes the results)
+  const long long nblocks =
+      fluid_list ? std::max(1LL, (c.nfluid + kStatSlots - 1) / kStatSlots)
+                 : (long long)grid.x * grid.y * grid.z;
+  // slot 0: the arrival counter; the block records; the results
+  const size_t need = (1 + (size_t)nblocks * ST_COUNT + ST_COUNT + 1) * sizeof(double);
   if (lat->stats_scratch_bytes < need) {
     // a larger area: earlier calls may still be reading the old one
     CUDA_TRY(cudaStreamSynchronize(lat->stream), "stats");
@@ -680,24 +683,28 @@ mlbm_status stats_enqueue(mlbm_lattice* lat, double* h) {
     lat->stats_scratch = nullptr;
     lat->stats_scratch_bytes = 0;
     CUDA_TRY(cudaMalloc((void**)&lat->stats_scratch, need), "stats scratch");
+    CUDA_TRY(cudaMemsetAsync(lat->stats_scratch, 0, sizeof(double), lat->stream),
+             "stats counter");
     lat->stats_scratch_bytes = need;
   }
-  double* partial = lat->stats_scratch;
-  double* fin = partial + (size_t)nblocks * ST_COUNT;
+  StatScratch sc;
+  sc.counter = reinterpret_cast<unsigned*>(lat->stats_scratch);
+  sc.records = lat->stats_scratch + 1;
+  sc.out = sc.records + (size_t)nblocks * ST_COUNT;
+  double* fin = sc.out;
   if (fluid_list) {
-    if (nblocks > 0)
-      k_stats_fluid<float><<<(unsigned)nblocks, kStatThreads, 0, lat->stream>>>(
-          static_cast<const float*>(lat->rho), c.cinfo, c.nfluid, lat->g,
-          lat->phys, partial);
-  } else if (lat->storage == MLBM_STORE_F64)
+    k_stats_fluid<float><<<(unsigned)nblocks, kStatThreads, 0, lat->stream>>>(
+        static_cast<const float*>(lat->rho), c.cinfo, c.nfluid, lat->g,
+        lat->phys, sc, lat->err);
+  } else if (lat->storage == MLBM_STORE_F64) {
     k_stats_partial<double><<<grid, dim3(32, 8), 0, lat->stream>>>(
-        static_cast<const double*>(lat->rho), lat->nbw, lat->g, lat->phys,
-        partial);
-  else
+        static_cast<const double*>(lat->rho), lat->nbw, lat->g, lat->phys, sc,
+        lat->err);
+  } else {
     k_stats_partial<float><<<grid, dim3(32, 8), 0, lat->stream>>>(
-        static_cast<const float*>(lat->rho), lat->nbw, lat->g, lat->phys,
-        partial);
-  k_stats_final<<<1, 256, 0, lat->stream>>>(partial, nblocks, lat->err, fin);
+        static_cast<const float*>(lat->rho), lat->nbw, lat->g, lat->phys, sc,
+        lat->err);
+  }
   CUDA_TRY(cudaGetLastError(), "stats launch");
   CUDA_TRY(cudaMemcpyAsync(h, fin, (ST_COUNT + 1) * sizeof(double),
                            cudaMemcpyDeviceToHost, lat->stream),

@@ -202,6 +202,26 @@ void own_range(const mlbm_lattice* lat, long long& kb, long long& ke) {
   }
 }
 
+// Launch a step kernel with programmatic stream serialization: it may begin
+// while the kernel before it in the stream finishes, and waits for it at
+// pdl_gate() (pair.cuh).
+template <typename... KArgs, typename... Args>
+void launch_overlapped(void (*kernel)(KArgs...), unsigned grid, cudaStream_t stream,
+                       Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(kC2Threads);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  // a failed launch is reported by the caller's cudaGetLastError
+  (void)cudaLaunchKernelEx(&cfg, kernel, args...);
+}
+
 unsigned c2_grid(long long kb, long long ke, long long per_thread) {
   const long long threads = (ke - kb + per_thread - 1) / per_thread;
   return (unsigned)((threads + kC2Threads - 1) / kC2Threads);
@@ -217,14 +237,10 @@ void launch_c2_density(mlbm_lattice* lat, const StepArgs& a, bool wr, bool inj,
   const uint32_t cs = (uint32_t)c.cs;
   float* rho = static_cast<float*>(lat->rho);
   float* psi = static_cast<float*>(lat->psi);
-  if (wr)
-    k_cdensity<T, PHASE, true><<<grid, kC2Threads, 0, lat->stream>>>(
-        cpop, cs, c.cinfo, c.wtab, (int)kb, (int)ke, rho, psi, lat->g, lat->phys,
-        a, inj);
-  else
-    k_cdensity<T, PHASE, false><<<grid, kC2Threads, 0, lat->stream>>>(
-        cpop, cs, c.cinfo, c.wtab, (int)kb, (int)ke, rho, psi, lat->g, lat->phys,
-        a, inj);
+  auto kernel = wr ? k_cdensity<T, PHASE, true> : k_cdensity<T, PHASE, false>;
+  launch_overlapped(kernel, grid, lat->stream, cpop, cs,
+                    (const uint2*)c.cinfo, (const uint2*)c.wtab, (int)kb,
+                    (int)ke, rho, psi, lat->g, lat->phys, a, inj);
 }
 
 template <typename T, int PHASE>
@@ -236,14 +252,10 @@ void launch_c2_update(mlbm_lattice* lat, const StepArgs& a, bool wu, bool inj,
   T* cpop = static_cast<T*>(c.cpop);
   const uint32_t cs = (uint32_t)c.cs;
   const float* psi = static_cast<const float*>(lat->psi);
-  if (wu)
-    k_cupdate<T, PHASE, true><<<grid, kC2Threads, 0, lat->stream>>>(
-        cpop, cs, c.cinfo, c.wtab, (int)kb, (int)ke, psi, lat->vel, lat->g,
-        lat->phys, a, inj);
-  else
-    k_cupdate<T, PHASE, false><<<grid, kC2Threads, 0, lat->stream>>>(
-        cpop, cs, c.cinfo, c.wtab, (int)kb, (int)ke, psi, lat->vel, lat->g,
-        lat->phys, a, inj);
+  auto kernel = wu ? k_cupdate<T, PHASE, true> : k_cupdate<T, PHASE, false>;
+  launch_overlapped(kernel, grid, lat->stream, cpop, cs, (const uint2*)c.cinfo,
+                    (const uint2*)c.wtab, (int)kb, (int)ke, psi, lat->vel,
+                    lat->g, lat->phys, a, inj);
 }
 
 bool inject_now(const mlbm_lattice* lat, const StepArgs& a) {

@@ -117,6 +117,9 @@ namespace mlbm {
 template <int PHASE>
 constexpr int c2_nodes_per_thread() { return PHASE == 0 ? 1 : 2; }
 
+// Both kernels pass pdl_gate() (pair.cuh): launched with programmatic
+// stream serialization, each overlaps its prologue with the end of the
+// kernel before it.
 template <typename T, int PHASE, bool WRITE_RHO>
 __global__ void __launch_bounds__(kC2Threads, 5)
     k_cdensity(const T* __restrict__ cpop, uint32_t cs,
@@ -127,11 +130,11 @@ __global__ void __launch_bounds__(kC2Threads, 5)
                                  ((long long)blockIdx.x * kC2Threads + threadIdx.x);
   if (k >= nfluid) return;
   if (PHASE == 0)
-    node_density0<T, WRITE_RHO>(cpop, cs, cinfo, wtab, (int)k, rho_out, psi, g,
-                                p, a, inj);
+    node_density0<T, WRITE_RHO, true>(cpop, cs, cinfo, wtab, (int)k, rho_out,
+                                      psi, g, p, a, inj);
   else
-    pair_density<T, 1, WRITE_RHO>(cpop, cs, cinfo, wtab, (int)k, nfluid,
-                                  rho_out, psi, g, p, a, inj);
+    pair_density<T, 1, WRITE_RHO, true>(cpop, cs, cinfo, wtab, (int)k, nfluid,
+                                        rho_out, psi, g, p, a, inj);
 }
 
 template <typename T, int PHASE, bool WRITE_U>
@@ -144,11 +147,12 @@ __global__ void __launch_bounds__(kC2Threads, 3)
                                  ((long long)blockIdx.x * kC2Threads + threadIdx.x);
   if (k >= nfluid) return;
   if (PHASE == 0)
-    node_update0<T, WRITE_U>(cpop, cs, cinfo, wtab, (int)k, PsiPlain{psi}, vel,
-                             g, p, a, inj);
+    node_update0<T, WRITE_U, PsiPlain, true>(cpop, cs, cinfo, wtab, (int)k,
+                                             PsiPlain{psi}, vel, g, p, a, inj);
   else
-    pair_update<T, 1, WRITE_U>(cpop, cs, cinfo, wtab, (int)k, nfluid,
-                               PsiPlain{psi}, vel, g, p, a, inj);
+    pair_update<T, 1, WRITE_U, PsiPlain, true>(cpop, cs, cinfo, wtab, (int)k,
+                                               nfluid, PsiPlain{psi}, vel, g,
+                                               p, a, inj);
 }
 
 }  // namespace mlbm

@@ -190,12 +190,69 @@ __device__ __forceinline__ void stat_block_reduce(double (&acc)[ST_COUNT],
   }
 }
 
+// Scratch of one statistics reduction (8-byte slots): slot 0 the arrival
+// counter (zero between calls), then the block records (ST_COUNT each),
+// then the ST_COUNT results and the device error flag.
+struct StatScratch {
+  unsigned* counter;
+  double* records;
+  double* out;
+};
+
+// Called by every thread of a block once the block's record is written
+// (stat_block_reduce).  The last block to arrive folds all records -- in a
+// fixed order, so the result does not depend on which block is last: thread
+// t folds records t, t + 256, ... ascending, then the warps' shuffle trees,
+// then the warps in order -- writes the results and the device error flag
+// and re-arms the counter.  Records are read through L2 (ld.global.cg):
+// other SMs wrote them.  256 threads.
+__device__ __forceinline__ void stat_last_block(StatScratch s, unsigned nblocks,
+                                                const int* __restrict__ err,
+                                                int tid) {
+  __shared__ bool last;
+  __shared__ double sh[kStatThreads / 32][ST_COUNT];
+  __threadfence();
+  __syncthreads();
+  if (tid == 0) last = atomicAdd(s.counter, 1u) == nblocks - 1;
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  double v[ST_COUNT];
+#pragma unroll
+  for (int k = 0; k < ST_COUNT; ++k) v[k] = stat_identity(k);
+  for (unsigned b = tid; b < nblocks; b += kStatThreads) {
+    const double* rec = s.records + (size_t)b * ST_COUNT;
+    double r[ST_COUNT];
+#pragma unroll
+    for (int k = 0; k < ST_COUNT; ++k) r[k] = __ldcg(rec + k);
+#pragma unroll
+    for (int k = 0; k < ST_COUNT; ++k) v[k] = stat_op(k, v[k], r[k]);
+  }
+#pragma unroll
+  for (int k = 0; k < ST_COUNT; ++k)
+    for (int off = 16; off > 0; off >>= 1)
+      v[k] = stat_op(k, v[k], __shfl_down_sync(0xffffffffu, v[k], off));
+  const int warp = tid >> 5, lane = tid & 31;
+  if (lane == 0)
+    for (int k = 0; k < ST_COUNT; ++k) sh[warp][k] = v[k];
+  __syncthreads();
+  if (tid < ST_COUNT) {
+    double r = sh[0][tid];
+    for (int w = 1; w < kStatThreads / 32; ++w) r = stat_op(tid, r, sh[w][tid]);
+    s.out[tid] = r;
+  }
+  if (tid == 0) {
+    s.out[ST_COUNT] = err ? (double)*err : 0.0;
+    *s.counter = 0u;
+  }
+}
+
 // Dense form: one block per 32 x 8 nodes of an (x, y) plane and kStatZ
 // planes; each thread folds its column of nodes, z ascending.
 template <typename R>
 __global__ void __launch_bounds__(kStatThreads)
     k_stats_partial(const R* __restrict__ rho, const uint32_t* __restrict__ nbw,
-                    Geom g, Phys p, double* __restrict__ partial) {
+                    Geom g, Phys p, StatScratch sc, const int* __restrict__ err) {
   double acc[ST_COUNT];
 #pragma unroll
   for (int k = 0; k < ST_COUNT; ++k) acc[k] = stat_identity(k);
@@ -227,7 +284,9 @@ __global__ void __launch_bounds__(kStatThreads)
   }
   const long long blk =
       blockIdx.x + (long long)gridDim.x * (blockIdx.y + (long long)gridDim.y * blockIdx.z);
-  stat_block_reduce(acc, threadIdx.y * 32 + threadIdx.x, partial + blk * ST_COUNT);
+  const int tid = threadIdx.y * 32 + threadIdx.x;
+  stat_block_reduce(acc, tid, sc.records + blk * ST_COUNT);
+  stat_last_block(sc, gridDim.x * gridDim.y * gridDim.z, err, tid);
 }
 
 // Fluid-list form, for a lattice held in the fluid-only layout: the threads
@@ -240,7 +299,8 @@ constexpr int kStatSlots = kStatThreads * kStatSlotsPerThread;
 template <typename R>
 __global__ void __launch_bounds__(kStatThreads)
     k_stats_fluid(const R* __restrict__ rho, const uint2* __restrict__ cinfo,
-                  long long nslots, Geom g, Phys p, double* __restrict__ partial) {
+                  long long nslots, Geom g, Phys p, StatScratch sc,
+                  const int* __restrict__ err) {
   double acc[ST_COUNT];
 #pragma unroll
   for (int k = 0; k < ST_COUNT; ++k) acc[k] = stat_identity(k);
@@ -270,38 +330,8 @@ __global__ void __launch_bounds__(kStatThreads)
                      (int)((ci[j].y >> 11) & 2047u), (int)(ci[j].y >> 22),
                      ci[j].x, rv[j]);
   }
-  stat_block_reduce(acc, threadIdx.x, partial + (long long)blockIdx.x * ST_COUNT);
-}
-
-// Reduce the per-block partials (fixed-order tree: deterministic) and append
-// the lattice's device error flag, so one copy brings both back.  Each thread
-// folds whole partial records (ST_COUNT independent loads per record), then
-// the block folds the threads' results pairwise.
-__global__ void __launch_bounds__(256)
-    k_stats_final(const double* __restrict__ partial, long long nblocks,
-                  const int* __restrict__ err, double* __restrict__ out) {
-  __shared__ double sh[ST_COUNT][256];
-  const int tid = threadIdx.x;
-  double v[ST_COUNT];
-#pragma unroll
-  for (int k = 0; k < ST_COUNT; ++k) v[k] = stat_identity(k);
-  for (long long b = tid; b < nblocks; b += 256) {
-    const double* rec = partial + b * ST_COUNT;
-#pragma unroll
-    for (int k = 0; k < ST_COUNT; ++k) v[k] = stat_op(k, v[k], __ldg(rec + k));
-  }
-#pragma unroll
-  for (int k = 0; k < ST_COUNT; ++k) sh[k][tid] = v[k];
-  __syncthreads();
-  for (int s = 128; s > 0; s >>= 1) {
-    if (tid < s)
-#pragma unroll
-      for (int k = 0; k < ST_COUNT; ++k)
-        sh[k][tid] = stat_op(k, sh[k][tid], sh[k][tid + s]);
-    __syncthreads();
-  }
-  if (tid < ST_COUNT) out[tid] = sh[tid][0];
-  if (tid == 0) out[ST_COUNT] = err ? (double)*err : 0.0;
+  stat_block_reduce(acc, threadIdx.x, sc.records + (long long)blockIdx.x * ST_COUNT);
+  stat_last_block(sc, gridDim.x, err, threadIdx.x);
 }
 
 // Per-x-plane fluid / liquid node counts (integer atomics: deterministic).

@@ -242,6 +242,23 @@ struct PsiPlain {
   __device__ __forceinline__ float nb(uint32_t i, int) const { return __ldg(psi + i); }
 };
 
+// Programmatic dependent launch.  A step kernel launched with the
+// programmatic-serialization attribute may start while the kernel before it
+// in the stream is still running; pdl_gate() waits until that kernel has
+// completed and its memory is visible (griddepcontrol.wait), then lets the
+// next kernel of the stream start the same way (launch_dependents).  Work
+// before the gate may only read what the kernel before does not write (the
+// node table, the AA addresses; in the update pass also the populations,
+// which the density pass only reads).  Without the attribute both
+// instructions return at once.
+template <bool PDL>
+__device__ __forceinline__ void pdl_gate() {
+  if (PDL) {
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+  }
+}
+
 // The two nodes of pair k (k even) and whether the second one exists.
 struct Pair {
   PairNode a, b;
@@ -260,7 +277,7 @@ __device__ __forceinline__ Pair load_pair(const uint2* __restrict__ cinfo, int k
 
 // Pre-collision populations of pair q (both phases), with the second lane a
 // copy of the first for a single-node pair.
-template <typename T, int PHASE>
+template <typename T, int PHASE, bool GATE = false>
 __device__ __forceinline__ void pair_load(const T* cpop, uint32_t cs,
                                           const uint2* __restrict__ wtab,
                                           const Geom& g, const Pair& q,
@@ -270,6 +287,7 @@ __device__ __forceinline__ void pair_load(const T* cpop, uint32_t cs,
     aa_addresses0(wtab, g, cs, q.a, A);
     aa_addresses0(wtab, g, cs, q.b, B);
   }
+  pdl_gate<GATE>();
   if (q.a.kind && q.b.kind) {
 #pragma unroll
     for (int i = 0; i < Q; ++i) f[i] = p_dup(0.f);
@@ -296,7 +314,7 @@ __device__ __forceinline__ float2 pair_rho(const Phys& p, const Geom& g,
 }
 
 // Density pass of one pair (the work of k_cdensity for two nodes).
-template <typename T, int PHASE, bool WRITE_RHO>
+template <typename T, int PHASE, bool WRITE_RHO, bool PDL = false>
 __device__ __forceinline__ void pair_density(const T* cpop, uint32_t cs,
                                              const uint2* __restrict__ cinfo,
                                              const uint2* __restrict__ wtab,
@@ -307,7 +325,7 @@ __device__ __forceinline__ void pair_density(const T* cpop, uint32_t cs,
   const Pair q = load_pair(cinfo, k, nfluid);
   uint32_t A[Q], B[Q];
   float2 f[Q];
-  pair_load<T, PHASE>(cpop, cs, wtab, g, q, p.rho_shift, A, B, f);
+  pair_load<T, PHASE, PDL>(cpop, cs, wtab, g, q, p.rho_shift, A, B, f);
   const float2 d = pair_rho(p, g, a, inj, q, f);
   if (WRITE_RHO) {
     rho_out[node_index(g, q.a.x, q.a.y, q.a.z)] = d.x;
@@ -318,7 +336,7 @@ __device__ __forceinline__ void pair_density(const T* cpop, uint32_t cs,
 }
 
 // Update pass of one pair (the work of k_cupdate for two nodes).
-template <typename T, int PHASE, bool WRITE_U, class PsiR>
+template <typename T, int PHASE, bool WRITE_U, class PsiR, bool PDL = false>
 __device__ __forceinline__ void pair_update(T* cpop, uint32_t cs,
                                             const uint2* __restrict__ cinfo,
                                             const uint2* __restrict__ wtab,
@@ -330,6 +348,7 @@ __device__ __forceinline__ void pair_update(T* cpop, uint32_t cs,
   uint32_t A[Q], B[Q];
   float2 f[Q];
   pair_load<T, PHASE>(cpop, cs, wtab, g, q, p.rho_shift, A, B, f);
+  pdl_gate<PDL>();  // psi and the population stores come from / go after it
   const float2 d = pair_rho(p, g, a, inj, q, f);
   float2 ux, uy, uz;
   {
@@ -375,7 +394,7 @@ __device__ __forceinline__ void pair_update(T* cpop, uint32_t cs,
 // per thread would double that, so this step runs one node per thread with
 // the scalar collide() of kernels.cuh (the same arithmetic, lane by lane, as
 // collide2).  Holes (no fluid bit) are skipped.
-template <typename T, bool WRITE_RHO>
+template <typename T, bool WRITE_RHO, bool PDL = false>
 __device__ __forceinline__ void node_density0(const T* cpop, uint32_t cs,
                                               const uint2* __restrict__ cinfo,
                                               const uint2* __restrict__ wtab,
@@ -386,10 +405,12 @@ __device__ __forceinline__ void node_density0(const T* cpop, uint32_t cs,
   if (!(n.nb & NB_SELF)) return;
   float d;
   if (n.kind) {
+    pdl_gate<PDL>();
     d = slab_density(p, n.kind);
   } else {
     uint32_t A[Q];
     aa_addresses0(wtab, g, cs, n, A);
+    pdl_gate<PDL>();
     float f[Q];
 #pragma unroll
     for (int e = 0; e < Q; ++e)
@@ -403,7 +424,7 @@ __device__ __forceinline__ void node_density0(const T* cpop, uint32_t cs,
   store_psi<float>(psi, g, n.x, n.y, n.z, psi_of<float>(p, d));
 }
 
-template <typename T, bool WRITE_U, class PsiR>
+template <typename T, bool WRITE_U, class PsiR, bool PDL = false>
 __device__ __forceinline__ void node_update0(T* cpop, uint32_t cs,
                                              const uint2* __restrict__ cinfo,
                                              const uint2* __restrict__ wtab,
@@ -419,10 +440,12 @@ __device__ __forceinline__ void node_update0(T* cpop, uint32_t cs,
   float ux = 0.f, uy = 0.f, uz = 0.f;
   if (n.kind) {
     slab_populations<float>(slab_density(p, n.kind), f);
+    pdl_gate<PDL>();
   } else {
 #pragma unroll
     for (int e = 0; e < Q; ++e)
       f[opp(e)] = PopPair<T>::ld1(cpop + A[e], shift * weight<float>(e));
+    pdl_gate<PDL>();  // psi and the population stores come from / go after it
     float d = 0.f;
 #pragma unroll
     for (int i = 0; i < Q; ++i) d = radd(d, f[i]);
