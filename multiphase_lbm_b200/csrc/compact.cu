@@ -246,7 +246,7 @@ void launch_c2_density(mlbm_lattice* lat, const StepArgs& a, bool wr, bool inj,
 template <typename T, int PHASE>
 void launch_c2_update(mlbm_lattice* lat, const StepArgs& a, bool wu, bool inj,
                       long long kb, long long ke) {
-  const unsigned grid = c2_grid(kb, ke, c2_nodes_per_thread<PHASE>());
+  const unsigned grid = c2_grid(kb, ke, c2_update_nodes_per_thread());
   if (grid == 0) return;
   const CompactState& c = lat->compact;
   T* cpop = static_cast<T*>(c.cpop);

@@ -106,16 +106,18 @@ static __global__ void k_wtab(const uint32_t* __restrict__ mask,
 
 namespace mlbm {
 
-// The local step (AA phase 1) runs one thread per pair of fluid nodes
-// (pair.cuh, k = 2 * thread index); the gather/push step (phase 0) one thread
-// per node (k = thread index), which keeps its neighbour addresses within a
-// register budget that leaves 3 CTAs per SM.  The density pass is held to 48
-// registers (5 CTAs per SM); on the 200^3 bench that beat 3, 4 and 6 CTAs
-// per SM for either pass.  Both kernels advance the compact indices
-// [kbeg, nfluid): the whole lattice, or the own planes of a slab lattice
-// (kbeg is a plane start, so it is even).
+// The update pass runs one thread per pair of fluid nodes (pair.cuh, k = 2 *
+// thread index) in both AA phases; the gather/push form (phase 0) keeps its
+// addresses in shared memory across the collision.  The density pass runs
+// pairs in the local phase and one node per thread in the gather phase
+// (pairs there measured 1 % slower: 38 live addresses at 64 registers).
+// The density pass is held to 48 registers (5 CTAs per SM); on the 200^3
+// bench that beat 3, 4 and 6 CTAs per SM.  Both kernels advance the compact
+// indices [kbeg, nfluid): the whole lattice, or the own planes of a slab
+// lattice (kbeg is a plane start, so it is even).
 template <int PHASE>
 constexpr int c2_nodes_per_thread() { return PHASE == 0 ? 1 : 2; }
+constexpr int c2_update_nodes_per_thread() { return 2; }
 
 // Both kernels pass pdl_gate() (pair.cuh): launched with programmatic
 // stream serialization, each overlaps its prologue with the end of the
@@ -143,16 +145,12 @@ __global__ void __launch_bounds__(kC2Threads, 3)
               const uint2* __restrict__ wtab, int kbeg, int nfluid,
               const float* __restrict__ psi, float* __restrict__ vel, Geom g,
               Phys p, StepArgs a, bool inj) {
-  const long long k = kbeg + c2_nodes_per_thread<PHASE>() *
+  const long long k = kbeg + c2_update_nodes_per_thread() *
                                  ((long long)blockIdx.x * kC2Threads + threadIdx.x);
   if (k >= nfluid) return;
-  if (PHASE == 0)
-    node_update0<T, WRITE_U, PsiPlain, true>(cpop, cs, cinfo, wtab, (int)k,
-                                             PsiPlain{psi}, vel, g, p, a, inj);
-  else
-    pair_update<T, 1, WRITE_U, PsiPlain, true>(cpop, cs, cinfo, wtab, (int)k,
-                                               nfluid, PsiPlain{psi}, vel, g,
-                                               p, a, inj);
+  pair_update<T, PHASE, WRITE_U, PsiPlain, true>(cpop, cs, cinfo, wtab, (int)k,
+                                                 nfluid, PsiPlain{psi}, vel, g,
+                                                 p, a, inj);
 }
 
 }  // namespace mlbm

@@ -347,7 +347,28 @@ __device__ __forceinline__ void pair_update(T* cpop, uint32_t cs,
   const Pair q = load_pair(cinfo, k, nfluid);
   uint32_t A[Q], B[Q];
   float2 f[Q];
-  pair_load<T, PHASE>(cpop, cs, wtab, g, q, p.rho_shift, A, B, f);
+  // The gather/push step (phase 0) parks its 2 x 19 addresses in shared
+  // memory between the gather and the push: held in registers across the
+  // collision they leave too few for 3 CTAs per SM.  Each node's addresses
+  // are parked right after its own gather, so only 19 are live at a time.
+  // (k_cupdate: 1-D blocks of kC2Threads.)
+  __shared__ uint32_t parked[PHASE == 0 ? 2 * Q : 1][PHASE == 0 ? kC2Threads : 1];
+  if (PHASE == 0) {
+    aa_addresses0(wtab, g, cs, q.a, A);
+#pragma unroll
+    for (int e = 0; e < Q; ++e) {
+      f[opp(e)].x = PopPair<T>::ld1(cpop + A[e], p.rho_shift * weight<float>(e));
+      parked[e][threadIdx.x] = A[e];
+    }
+    aa_addresses0(wtab, g, cs, q.b, A);  // q.b is q.a for a one-node pair
+#pragma unroll
+    for (int e = 0; e < Q; ++e) {
+      f[opp(e)].y = PopPair<T>::ld1(cpop + A[e], p.rho_shift * weight<float>(e));
+      parked[Q + e][threadIdx.x] = A[e];
+    }
+  } else {
+    pair_load<T, PHASE>(cpop, cs, wtab, g, q, p.rho_shift, A, B, f);
+  }
   pdl_gate<PDL>();  // psi and the population stores come from / go after it
   const float2 d = pair_rho(p, g, a, inj, q, f);
   float2 ux, uy, uz;
@@ -384,16 +405,25 @@ __device__ __forceinline__ void pair_update(T* cpop, uint32_t cs,
     vel[3 * nb + 1] = uy.y;
     vel[3 * nb + 2] = uz.y;
   }
+  if (PHASE == 0) {
+    const volatile uint32_t(*pk)[PHASE == 0 ? kC2Threads : 1] = parked;
+#pragma unroll
+    for (int e = 0; e < Q; ++e) {
+      A[e] = pk[e][threadIdx.x];
+      B[e] = pk[Q + e][threadIdx.x];
+    }
+  }
   pair_scatter<T, PHASE>(cpop, cs, k, A, B, p.rho_shift, f);
 }
 
 
 
 // ---- one node per thread (AA phase 0) -----------------------------------------
-// The gather/push step keeps 18 neighbour addresses per node live; two nodes
-// per thread would double that, so this step runs one node per thread with
-// the scalar collide() of kernels.cuh (the same arithmetic, lane by lane, as
-// collide2).  Holes (no fluid bit) are skipped.
+// The density pass of the gather step (k_cdensity), and the gather/push
+// update of the batch kernels (batch_compact.cuh, whose blocks hold several
+// domains), one node per thread with the scalar collide() of kernels.cuh
+// (the same arithmetic, lane by lane, as collide2).  Holes (no fluid bit)
+// are skipped.
 template <typename T, bool WRITE_RHO, bool PDL = false>
 __device__ __forceinline__ void node_density0(const T* cpop, uint32_t cs,
                                               const uint2* __restrict__ cinfo,
@@ -424,7 +454,7 @@ __device__ __forceinline__ void node_density0(const T* cpop, uint32_t cs,
   store_psi<float>(psi, g, n.x, n.y, n.z, psi_of<float>(p, d));
 }
 
-template <typename T, bool WRITE_U, class PsiR, bool PDL = false>
+template <typename T, bool WRITE_U, class PsiR>
 __device__ __forceinline__ void node_update0(T* cpop, uint32_t cs,
                                              const uint2* __restrict__ cinfo,
                                              const uint2* __restrict__ wtab,
@@ -440,12 +470,10 @@ __device__ __forceinline__ void node_update0(T* cpop, uint32_t cs,
   float ux = 0.f, uy = 0.f, uz = 0.f;
   if (n.kind) {
     slab_populations<float>(slab_density(p, n.kind), f);
-    pdl_gate<PDL>();
   } else {
 #pragma unroll
     for (int e = 0; e < Q; ++e)
       f[opp(e)] = PopPair<T>::ld1(cpop + A[e], shift * weight<float>(e));
-    pdl_gate<PDL>();  // psi and the population stores come from / go after it
     float d = 0.f;
 #pragma unroll
     for (int i = 0; i < Q; ++i) d = radd(d, f[i]);
