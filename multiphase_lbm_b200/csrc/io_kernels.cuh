@@ -139,24 +139,14 @@ __device__ __forceinline__ void stat_node(double (&acc)[ST_COUNT],
     acc[ST_NL] += 1.0;
     acc[ST_PL] += (double)pr;
     acc[ST_RL] += (double)r;
+    Nbr a;
+    a.init(g, x, y, z);
     // all 18 neighbour densities as independent loads (every periodic
     // index lies inside the array, solid nodes included), then the masks:
-    // a load under each direction's branch would wait on the one before.
-    // A node off every boundary face needs no periodic wrap.
+    // a load under each direction's branch would wait on the one before
     R nr[Q];
-    if ((unsigned)(x - 1) < (unsigned)(g.lx - 2) &&
-        (unsigned)(y - 1) < (unsigned)(g.ly - 2) &&
-        (unsigned)(z - 1) < (unsigned)(g.lz - 2)) {
-      const R* c = rho + node_index(g, x, y, z);
-      const int px = g.px, pz = g.ly * g.px;
 #pragma unroll
-      for (int i = 1; i < Q; ++i) nr[i] = __ldg(c - (ex(i) + ey(i) * px + ez(i) * pz));
-    } else {
-      Nbr a;
-      a.init(g, x, y, z);
-#pragma unroll
-      for (int i = 1; i < Q; ++i) nr[i] = __ldg(rho + a.idx(-ex(i), -ey(i), -ez(i)));
-    }
+    for (int i = 1; i < Q; ++i) nr[i] = __ldg(rho + a.idx(-ex(i), -ey(i), -ez(i)));
     const uint32_t solid = ~nb & 0x7fffeu;  // directions 1..18
     uint32_t low = 0u;
 #pragma unroll

@@ -70,17 +70,10 @@ __host__ __device__ __forceinline__ long long psi_elems(const Geom& g) {
   return (long long)(g.lz + 2) * (g.ly + 2) * g.pxg;
 }
 
-// Store psi of node (x, y, z) and its periodic ghost copies (a node off
-// every boundary face has none: one store).
+// Store psi of node (x, y, z) and its periodic ghost copies.
 template <typename R>
 __device__ __forceinline__ void store_psi(R* __restrict__ psi, const Geom& g,
                                           int x, int y, int z, R v) {
-  if ((unsigned)(x - 1) < (unsigned)(g.lx - 2) &&
-      (unsigned)(y - 1) < (unsigned)(g.ly - 2) &&
-      (unsigned)(z - 1) < (unsigned)(g.lz - 2)) {
-    psi[psi_index(g, x, y, z)] = v;
-    return;
-  }
   const int xs[3] = {x, x == 0 ? g.lx : INT_MIN, x == g.lx - 1 ? -1 : INT_MIN};
   const int ys[3] = {y, y == 0 ? g.ly : INT_MIN, y == g.ly - 1 ? -1 : INT_MIN};
   const int zs[3] = {z, z == 0 ? g.lz : INT_MIN, z == g.lz - 1 ? -1 : INT_MIN};
