@@ -42,9 +42,11 @@ struct mlbm_batch {
   // pass is one launch over all of them (batch_compact.cuh)
   bool compact = false;
   CDomain* d_cdesc = nullptr;
-  long long* d_cpre = nullptr;  // [2][n + 1] block prefixes per step parity
+  // block prefixes: [2][n + 1] of the density pass per step parity, then
+  // [n + 1] of the update pass (node pairs in both AA phases)
+  long long* d_cpre = nullptr;
   int ccap = 0;
-  int grid_c = 0;
+  int grid_c = 0, grid_cu = 0;
 };
 
 namespace {
@@ -85,12 +87,14 @@ const void* pick_update(int storage) {
 }
 
 // Compact mode: every domain enters the fluid-only layout; block prefixes
-// for both step parities (one node per thread in the gather/push step, one
-// pair per thread in the local step).
+// of the density pass for both step parities (one node per thread in the
+// gather step, one pair per thread in the local step) and of the update
+// pass (one pair per thread in both).
 mlbm_status rebuild_compact(mlbm_batch* b) {
   std::vector<CDomain> desc;
   std::vector<long long> pre[2] = {std::vector<long long>(1, 0),
                                    std::vector<long long>(1, 0)};
+  std::vector<long long> upre(1, 0);
   for (size_t s = 0; s < b->dom.size(); ++s) {
     mlbm_lattice* lat = b->dom[s];
     if (!lat) continue;
@@ -115,6 +119,7 @@ mlbm_status rebuild_compact(mlbm_batch* b) {
       const long long threads = ph == 0 ? d.nfluid : d.nfluid / 2;
       pre[par].push_back(pre[par].back() + (threads + kBCThreads - 1) / kBCThreads);
     }
+    upre.push_back(upre.back() + (d.nfluid / 2 + kBCThreads - 1) / kBCThreads);
   }
   const int n = (int)desc.size();
   if (n > kMaxBatch) return bfail(MLBM_ERR_ARG, "too many domains in a batch");
@@ -125,11 +130,12 @@ mlbm_status rebuild_compact(mlbm_batch* b) {
     b->d_cpre = nullptr;
     const int cap = std::max(n, 64);
     BCUDA(cudaMalloc(&b->d_cdesc, cap * sizeof(CDomain)), "batch table");
-    BCUDA(cudaMalloc(&b->d_cpre, 2 * (cap + 1) * sizeof(long long)), "batch table");
+    BCUDA(cudaMalloc(&b->d_cpre, 3 * (cap + 1) * sizeof(long long)), "batch table");
     b->ccap = cap;
   }
   std::vector<long long> both(pre[0]);
   both.insert(both.end(), pre[1].begin(), pre[1].end());
+  both.insert(both.end(), upre.begin(), upre.end());
   if (n)
     BCUDA(cudaMemcpyAsync(b->d_cdesc, desc.data(), n * sizeof(CDomain),
                           cudaMemcpyHostToDevice, b->stream), "batch table");
@@ -140,6 +146,7 @@ mlbm_status rebuild_compact(mlbm_batch* b) {
   BCUDA(cudaStreamSynchronize(b->stream), "batch table");
   b->nactive = n;
   b->grid_c = (int)std::max<long long>(1, std::max(pre[0].back(), pre[1].back()));
+  b->grid_cu = (int)std::max<long long>(1, upre.back());
   b->dirty = false;
   return MLBM_OK;
 }
@@ -239,8 +246,9 @@ void launch_step(mlbm_batch* b, int delta, int reverse, unsigned inject,
       else
         k_batch_cdensity<T, false><<<b->grid_c, kBCThreads, 0, b->stream>>>(
             b->d_cdesc, b->d_cpre, b->nactive, b->d_step, delta, reverse, inject);
-      k_batch_cupdate<T><<<b->grid_c, kBCThreads, 0, b->stream>>>(
-          b->d_cdesc, b->d_cpre, b->nactive, b->d_step, delta, reverse, inject);
+      k_batch_cupdate<T><<<b->grid_cu, kBCThreads, 0, b->stream>>>(
+          b->d_cdesc, b->d_cpre + 2 * (b->nactive + 1), b->nactive, b->d_step,
+          delta, reverse, inject);
       return;
     }
   }

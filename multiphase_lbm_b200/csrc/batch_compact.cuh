@@ -5,12 +5,13 @@
 // same domain advanced alone.
 //
 // Each domain owns a contiguous range of blocks.  The AA phase of a domain
-// at batch step s is phase_base ^ (s & 1); the gather/push step runs one
-// node per thread and the local step one pair per thread, so a domain's
-// block count depends on the parity of s: there are two block-prefix tables,
-// one per parity, and the launch grid covers the larger total.  The batch
-// step s is read from the device counter (graph replays advance it), so a
-// captured graph stays valid for every start parity.
+// at batch step s is phase_base ^ (s & 1).  The density pass runs one node
+// per thread in the gather step and one pair per thread in the local step,
+// so a domain's block count depends on the parity of s: two block-prefix
+// tables, one per parity, and the launch grid covers the larger total.  The
+// update pass runs one pair per thread in both phases (one table).  The
+// batch step s is read from the device counter (graph replays advance it),
+// so a captured graph stays valid for every start parity.
 #pragma once
 
 #include "batch.cuh"
@@ -81,31 +82,34 @@ __global__ void __launch_bounds__(kBCThreads, 3)
   }
 }
 
+// upre: the update pass's block prefixes (n + 1 entries, both parities).
+// Blocks of kBCThreads = kC2Threads threads, as pair_update's phase-0 form
+// requires.
 template <typename T>
 __global__ void __launch_bounds__(kBCThreads, 3)
     k_batch_cupdate(const CDomain* __restrict__ doms,
-                    const long long* __restrict__ pre, int n,
+                    const long long* __restrict__ upre, int n,
                     const long long* __restrict__ step, int delta, int reverse,
                     unsigned inject_type) {
+  static_assert(kBCThreads == kC2Threads, "pair_update's parked addresses");
   const long long s = *step + delta;
-  int d;
-  long long local;
-  if (!bc_locate(pre, n, s, d, local)) return;
+  const long long b = blockIdx.x;
+  if (b >= upre[n]) return;
+  const int d = find_domain(upre, n, b);
   const CDomain& D = doms[d];
   const int ph = D.phase_base ^ (int)(s & 1);
   StepArgs a{s - D.step_origin, reverse, inject_type};
   const bool inj = bc_inject(D.p, a.step);
-  const long long t = local * kBCThreads + threadIdx.x;
-  if (ph == 0) {
-    if (t >= D.nfluid) return;
-    node_update0<T, false>(static_cast<T*>(D.cpop), D.cs, D.cinfo, D.wtab,
-                           (int)t, PsiPlain{D.psi}, nullptr, D.g, D.p, a, inj);
-  } else {
-    if (2 * t >= D.nfluid) return;
+  const long long k = 2 * ((b - upre[d]) * kBCThreads + threadIdx.x);
+  if (k >= D.nfluid) return;
+  if (ph == 0)
+    pair_update<T, 0, false>(static_cast<T*>(D.cpop), D.cs, D.cinfo, D.wtab,
+                             (int)k, D.nfluid, PsiPlain{D.psi}, nullptr, D.g,
+                             D.p, a, inj);
+  else
     pair_update<T, 1, false>(static_cast<T*>(D.cpop), D.cs, D.cinfo, D.wtab,
-                             (int)(2 * t), D.nfluid, PsiPlain{D.psi}, nullptr,
-                             D.g, D.p, a, inj);
-  }
+                             (int)k, D.nfluid, PsiPlain{D.psi}, nullptr, D.g,
+                             D.p, a, inj);
 }
 
 }  // namespace mlbm

@@ -419,11 +419,8 @@ __device__ __forceinline__ void pair_update(T* cpop, uint32_t cs,
 
 
 // ---- one node per thread (AA phase 0) -----------------------------------------
-// The density pass of the gather step (k_cdensity), and the gather/push
-// update of the batch kernels (batch_compact.cuh, whose blocks hold several
-// domains), one node per thread with the scalar collide() of kernels.cuh
-// (the same arithmetic, lane by lane, as collide2).  Holes (no fluid bit)
-// are skipped.
+// The density pass of the gather step: one node per thread (on pairs its 38
+// live addresses measured slower).  Holes (no fluid bit) are skipped.
 template <typename T, bool WRITE_RHO, bool PDL = false>
 __device__ __forceinline__ void node_density0(const T* cpop, uint32_t cs,
                                               const uint2* __restrict__ cinfo,
@@ -452,49 +449,6 @@ __device__ __forceinline__ void node_density0(const T* cpop, uint32_t cs,
   }
   if (WRITE_RHO) rho_out[node_index(g, n.x, n.y, n.z)] = d;
   store_psi<float>(psi, g, n.x, n.y, n.z, psi_of<float>(p, d));
-}
-
-template <typename T, bool WRITE_U, class PsiR>
-__device__ __forceinline__ void node_update0(T* cpop, uint32_t cs,
-                                             const uint2* __restrict__ cinfo,
-                                             const uint2* __restrict__ wtab,
-                                             int k, const PsiR& pr, float* vel,
-                                             const Geom& g, const Phys& p,
-                                             const StepArgs& a, bool inj) {
-  const PairNode n = pair_node(cinfo, k);
-  if (!(n.nb & NB_SELF)) return;
-  const float shift = p.rho_shift;
-  uint32_t A[Q];
-  aa_addresses0(wtab, g, cs, n, A);
-  float f[Q];
-  float ux = 0.f, uy = 0.f, uz = 0.f;
-  if (n.kind) {
-    slab_populations<float>(slab_density(p, n.kind), f);
-  } else {
-#pragma unroll
-    for (int e = 0; e < Q; ++e)
-      f[opp(e)] = PopPair<T>::ld1(cpop + A[e], shift * weight<float>(e));
-    float d = 0.f;
-#pragma unroll
-    for (int i = 0; i < Q; ++i) d = radd(d, f[i]);
-    d = inject_on(p, g, a, inj, n.y, d);
-    const uint32_t pc = (uint32_t)psi_index(g, n.x, n.y, n.z);
-    const int sy = g.pxg, sz = (g.ly + 2) * g.pxg;
-    pr.ready();
-    collide<float>(
-        p, d, pr.self(pc),
-        [&](int i) { return pr.nb(pc + (ex(i) + ey(i) * sy + ez(i) * sz), i); },
-        f, ux, uy, uz);
-  }
-  if (WRITE_U) {
-    const long long m = node_index(g, n.x, n.y, n.z);
-    vel[3 * m] = ux;
-    vel[3 * m + 1] = uy;
-    vel[3 * m + 2] = uz;
-  }
-#pragma unroll
-  for (int e = 0; e < Q; ++e)
-    PopPair<T>::st1(cpop + A[e], f[e], shift * weight<float>(e));
 }
 
 }  // namespace mlbm
