@@ -2,7 +2,7 @@
 
 The oracle is ``oracle/mlbm_oracle.c`` (a C restatement that reproduces the
 reference's own kernels bit for bit, see test_oracle_pin.py) on the same
-seeded inputs.  Tolerances (BASELINE parity bar):
+seeded inputs.  Tolerances (the parity bar of the FP32 drop-in):
   * FP32 storage: density within 1e-5 relative (pointwise over fluid nodes)
     and populations / velocity within 1e-5 relative to their largest value,
     over the first 100 steps;
