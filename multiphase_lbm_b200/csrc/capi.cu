@@ -669,11 +669,27 @@ mlbm_status stats_enqueue(mlbm_lattice* lat, double* h) {
   const bool fluid_list = c.active && c.cinfo && lat->storage != MLBM_STORE_F64;
   const dim3 grid(lat->g.px / 32, (lat->g.ly + 7) / 8,
                   (lat->g.lz + kStatZ - 1) / kStatZ);
-  // (the fluid-list form launches one block at least: the last block to
-  // finish writes the results)
-  const long long nblocks =
-      fluid_list ? std::max(1LL, (c.nfluid + kStatSlots - 1) / kStatSlots)
-                 : (long long)grid.x * grid.y * grid.z;
+  // The fluid-list form runs one wave of resident blocks over even spans of
+  // the node table (spans of whole 256-slot rounds; one block at least: the
+  // last block to finish writes the results).
+  long long nblocks = (long long)grid.x * grid.y * grid.z, span = 0;
+  if (fluid_list) {
+    if (lat->stats_wave <= 0) {
+      int per_sm = 0, nsm = 0;
+      CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+                   &per_sm, k_stats_fluid<float>, kStatThreads, 0),
+               "stats occupancy");
+      CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount,
+                                      lat->device),
+               "stats occupancy");
+      lat->stats_wave = std::max(1, per_sm * nsm);
+    }
+    const long long rounds =
+        std::max(1LL, (c.nfluid + kStatThreads - 1) / kStatThreads);
+    nblocks = std::min<long long>(lat->stats_wave, rounds);
+    span = (rounds + nblocks - 1) / nblocks * kStatThreads;
+    nblocks = std::max(1LL, (c.nfluid + span - 1) / span);
+  }
   // slot 0: the arrival counter; the block records; the results
   const size_t need = (1 + (size_t)nblocks * ST_COUNT + ST_COUNT + 1) * sizeof(double);
   if (lat->stats_scratch_bytes < need) {
@@ -694,7 +710,7 @@ mlbm_status stats_enqueue(mlbm_lattice* lat, double* h) {
   double* fin = sc.out;
   if (fluid_list) {
     k_stats_fluid<float><<<(unsigned)nblocks, kStatThreads, 0, lat->stream>>>(
-        static_cast<const float*>(lat->rho), c.cinfo, c.nfluid, lat->g,
+        static_cast<const float*>(lat->rho), c.cinfo, c.nfluid, span, lat->g,
         lat->phys, sc, lat->err);
   } else if (lat->storage == MLBM_STORE_F64) {
     k_stats_partial<double><<<grid, dim3(32, 8), 0, lat->stream>>>(

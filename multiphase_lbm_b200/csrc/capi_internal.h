@@ -59,6 +59,7 @@ struct mlbm_lattice {
   size_t staging_bytes = 0;
   double* stats_scratch = nullptr;
   size_t stats_scratch_bytes = 0;
+  int stats_wave = 0;           // resident blocks of the statistics kernel
 
   // update pass: z-march tiles and the TMA descriptor of the psi tensor
   mlbm::ZMarch zm{};

@@ -107,13 +107,16 @@ template <typename T>
 mlbm_status enter_t(mlbm_lattice* lat) {
   CompactState& c = lat->compact;
   const CArgs a = args_of(lat);
-  k_convert<T, true><<<node_grid(lat->g), node_block(), 0, lat->stream>>>(
-      static_cast<T*>(lat->pop), static_cast<T*>(c.cpop), a, lat->g);
   // holes keep (0, 0): no fluid bit
   cudaError_t e = cudaMemsetAsync(c.cinfo, 0, c.cs * sizeof(uint2), lat->stream);
   if (e != cudaSuccess) return cuda_fail(e, "compact node table");
   k_cinfo<<<node_grid(lat->g), node_block(), 0, lat->stream>>>(lat->nbw, c.cinfo,
                                                                 a, lat->g);
+  // the layout change comes last: the first step's density pass, launched
+  // with programmatic dependent launch, reads the node table before it
+  // waits for the kernel before it (launch_overlapped)
+  k_convert<T, true><<<node_grid(lat->g), node_block(), 0, lat->stream>>>(
+      static_cast<T*>(lat->pop), static_cast<T*>(c.cpop), a, lat->g);
   e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(e, "compact entry launch");
   return MLBM_OK;
@@ -202,12 +205,22 @@ void own_range(const mlbm_lattice* lat, long long& kb, long long& ke) {
   }
 }
 
-// Launch a step kernel with programmatic stream serialization: it may begin
-// while the kernel before it in the stream finishes, and waits for it at
-// pdl_gate() (pair.cuh).
+// Launch a step kernel, with programmatic stream serialization when
+// `overlap`: it may then begin while the kernel before it in the stream
+// finishes, and waits for it at pdl_gate() (pair.cuh).  What a kernel reads
+// before its gate must not be written by the kernel launched right before
+// it, whose writes are visible only after the gate:
+//   k_cdensity reads the node table (cinfo, wtab) before its gate; the
+//     tables are written only in compact_enter, whose last kernel
+//     (k_convert) does not write them;
+//   k_cupdate also gathers populations before its gate; it is launched with
+//     overlap only right after the density pass of the same step
+//     (launch_compact_two_pass), which reads them only.  The slab pass API
+//     (launch_compact_pass) may run halo moves between the passes, so it
+//     launches without overlap.
 template <typename... KArgs, typename... Args>
-void launch_overlapped(void (*kernel)(KArgs...), unsigned grid, cudaStream_t stream,
-                       Args... args) {
+void launch_overlapped(bool overlap, void (*kernel)(KArgs...), unsigned grid,
+                       cudaStream_t stream, Args... args) {
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(grid);
   cfg.blockDim = dim3(kC2Threads);
@@ -217,7 +230,7 @@ void launch_overlapped(void (*kernel)(KArgs...), unsigned grid, cudaStream_t str
   attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
   attr[0].val.programmaticStreamSerializationAllowed = 1;
   cfg.attrs = attr;
-  cfg.numAttrs = 1;
+  cfg.numAttrs = overlap ? 1 : 0;
   // a failed launch is reported by the caller's cudaGetLastError
   (void)cudaLaunchKernelEx(&cfg, kernel, args...);
 }
@@ -229,7 +242,7 @@ unsigned c2_grid(long long kb, long long ke, long long per_thread) {
 
 template <typename T, int PHASE>
 void launch_c2_density(mlbm_lattice* lat, const StepArgs& a, bool wr, bool inj,
-                       long long kb, long long ke) {
+                       long long kb, long long ke, bool overlap) {
   const CompactState& c = lat->compact;
   const unsigned grid = c2_grid(kb, ke, c2_nodes_per_thread<PHASE>());
   if (grid == 0) return;
@@ -238,14 +251,14 @@ void launch_c2_density(mlbm_lattice* lat, const StepArgs& a, bool wr, bool inj,
   float* rho = static_cast<float*>(lat->rho);
   float* psi = static_cast<float*>(lat->psi);
   auto kernel = wr ? k_cdensity<T, PHASE, true> : k_cdensity<T, PHASE, false>;
-  launch_overlapped(kernel, grid, lat->stream, cpop, cs,
+  launch_overlapped(overlap, kernel, grid, lat->stream, cpop, cs,
                     (const uint2*)c.cinfo, (const uint2*)c.wtab, (int)kb,
                     (int)ke, rho, psi, lat->g, lat->phys, a, inj);
 }
 
 template <typename T, int PHASE>
 void launch_c2_update(mlbm_lattice* lat, const StepArgs& a, bool wu, bool inj,
-                      long long kb, long long ke) {
+                      long long kb, long long ke, bool overlap) {
   const unsigned grid = c2_grid(kb, ke, c2_update_nodes_per_thread());
   if (grid == 0) return;
   const CompactState& c = lat->compact;
@@ -253,7 +266,8 @@ void launch_c2_update(mlbm_lattice* lat, const StepArgs& a, bool wu, bool inj,
   const uint32_t cs = (uint32_t)c.cs;
   const float* psi = static_cast<const float*>(lat->psi);
   auto kernel = wu ? k_cupdate<T, PHASE, true> : k_cupdate<T, PHASE, false>;
-  launch_overlapped(kernel, grid, lat->stream, cpop, cs, (const uint2*)c.cinfo,
+  launch_overlapped(overlap, kernel, grid, lat->stream, cpop, cs,
+                    (const uint2*)c.cinfo,
                     (const uint2*)c.wtab, (int)kb, (int)ke, psi, lat->vel,
                     lat->g, lat->phys, a, inj);
 }
@@ -272,11 +286,11 @@ mlbm_status launch_compact_two_pass(mlbm_lattice* lat, const StepArgs& a,
   long long kb, ke;
   own_range(lat, kb, ke);
   if (lat->phase == 0) {
-    launch_c2_density<T, 0>(lat, a, write_rho, inj, kb, ke);
-    launch_c2_update<T, 0>(lat, a, write_u, inj, kb, ke);
+    launch_c2_density<T, 0>(lat, a, write_rho, inj, kb, ke, true);
+    launch_c2_update<T, 0>(lat, a, write_u, inj, kb, ke, true);
   } else {
-    launch_c2_density<T, 1>(lat, a, write_rho, inj, kb, ke);
-    launch_c2_update<T, 1>(lat, a, write_u, inj, kb, ke);
+    launch_c2_density<T, 1>(lat, a, write_rho, inj, kb, ke, true);
+    launch_c2_update<T, 1>(lat, a, write_u, inj, kb, ke, true);
   }
   const cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(e, "compact two-pass launch");
@@ -295,13 +309,13 @@ mlbm_status launch_compact_pass(mlbm_lattice* lat, const StepArgs& a, int pass,
   if (pass == 0) {
     long long kb, ke;
     own_range(lat, kb, ke);
-    if (lat->phase == 0) launch_c2_density<T, 0>(lat, a, write_rho, inj, kb, ke);
-    else launch_c2_density<T, 1>(lat, a, write_rho, inj, kb, ke);
+    if (lat->phase == 0) launch_c2_density<T, 0>(lat, a, write_rho, inj, kb, ke, false);
+    else launch_c2_density<T, 1>(lat, a, write_rho, inj, kb, ke, false);
   } else {
     long long kb, ke;
     own_range(lat, kb, ke);
-    if (lat->phase == 0) launch_c2_update<T, 0>(lat, a, write_u, inj, kb, ke);
-    else launch_c2_update<T, 1>(lat, a, write_u, inj, kb, ke);
+    if (lat->phase == 0) launch_c2_update<T, 0>(lat, a, write_u, inj, kb, ke, false);
+    else launch_c2_update<T, 1>(lat, a, write_u, inj, kb, ke, false);
   }
   const cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(e, "compact pass launch");

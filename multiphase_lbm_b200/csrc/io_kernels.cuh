@@ -291,29 +291,29 @@ __global__ void __launch_bounds__(kStatThreads)
 
 // Fluid-list form, for a lattice held in the fluid-only layout: the threads
 // walk the compact node table (node word, packed x, y, z), so no lane idles
-// on a solid node.  Block b folds slots [b * kStatSlots, (b + 1) *
-// kStatSlots); thread t takes slots t, t + 256, ... of them, ascending.
-constexpr int kStatSlotsPerThread = 16;
-constexpr int kStatSlots = kStatThreads * kStatSlotsPerThread;
-
+// on a solid node.  The grid is one wave of resident blocks (the host sizes
+// it); block b folds slots [b * span, (b + 1) * span) and thread t takes
+// slots t, t + 256, ... of them, ascending -- a fixed assignment, so the
+// sums do not depend on scheduling.
 template <typename R>
 __global__ void __launch_bounds__(kStatThreads)
     k_stats_fluid(const R* __restrict__ rho, const uint2* __restrict__ cinfo,
-                  long long nslots, Geom g, Phys p, StatScratch sc,
-                  const int* __restrict__ err) {
+                  long long nslots, long long span, Geom g, Phys p,
+                  StatScratch sc, const int* __restrict__ err) {
   double acc[ST_COUNT];
 #pragma unroll
   for (int k = 0; k < ST_COUNT; ++k) acc[k] = stat_identity(k);
-  const long long base = (long long)blockIdx.x * kStatSlots + threadIdx.x;
+  const long long b0 = (long long)blockIdx.x * span;
+  const long long end = min(b0 + span, nslots);
   constexpr int U = 8;
 #pragma unroll 1
-  for (int j0 = 0; j0 < kStatSlotsPerThread; j0 += U) {
+  for (long long k0 = b0 + threadIdx.x; k0 < end; k0 += (long long)U * kStatThreads) {
     uint2 ci[U];
     R rv[U];
 #pragma unroll
     for (int j = 0; j < U; ++j) {
-      const long long k = base + (long long)(j0 + j) * kStatThreads;
-      ci[j] = k < nslots ? __ldg(cinfo + k) : make_uint2(0u, 0u);
+      const long long k = k0 + (long long)j * kStatThreads;
+      ci[j] = k < end ? __ldg(cinfo + k) : make_uint2(0u, 0u);
     }
 #pragma unroll
     for (int j = 0; j < U; ++j) {
