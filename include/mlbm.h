@@ -177,8 +177,11 @@ mlbm_status mlbm_iterate(mlbm_lattice* lat, int64_t step0, int32_t nsteps,
  *                dense layout; bit-identical to the reference's kernels;
  *   COMPACT      the two passes over a fluid-only population layout (solid
  *                nodes own no population storage), one thread per fluid
- *                node pair; bit-identical to TWO_PASS.  FP32 / FP16 storage,
- *                at most 2048 x 2048 x 1024 nodes;
+ *                node pair (one per node in the gather step's density
+ *                pass), each launch overlapping the end of the one before
+ *                (programmatic dependent launch); bit-identical to
+ *                TWO_PASS.  FP32 / FP16 storage, at most 2048 x 2048 x 1024
+ *                nodes;
  *   BAND         ONE launch per step over the fluid-only layout with two
  *                population buffers: the launch reads the step's
  *                populations from one buffer and pushes the new ones into
