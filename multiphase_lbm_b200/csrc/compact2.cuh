@@ -110,7 +110,7 @@ namespace mlbm {
 // thread index) in both AA phases; the gather/push form (phase 0) keeps its
 // addresses in shared memory across the collision.  The density pass runs
 // pairs in the local phase and one node per thread in the gather phase
-// (pairs there measured 1 % slower: 38 live addresses at 64 registers).
+// (pairs there measured 1 % slower at 64 and at 80 registers).
 // The density pass is held to 48 registers (5 CTAs per SM); on the 200^3
 // bench that beat 3, 4 and 6 CTAs per SM.  Both kernels advance the compact
 // indices [kbeg, nfluid): the whole lattice, or the own planes of a slab

@@ -419,8 +419,9 @@ __device__ __forceinline__ void pair_update(T* cpop, uint32_t cs,
 
 
 // ---- one node per thread (AA phase 0) -----------------------------------------
-// The density pass of the gather step: one node per thread (on pairs its 38
-// live addresses measured slower).  Holes (no fluid bit) are skipped.
+// The density pass of the gather step: one node per thread (on pairs it
+// measured slower at 64 and at 80 registers).  Holes (no fluid bit) are
+// skipped.
 template <typename T, bool WRITE_RHO, bool PDL = false>
 __device__ __forceinline__ void node_density0(const T* cpop, uint32_t cs,
                                               const uint2* __restrict__ cinfo,
