@@ -20,7 +20,7 @@ form is timed in the same run (``fp16``).  ``e2e`` is the same metric
 through the C ABI with host buffers: geometry and initial density copied in
 from pinned host memory, then every step an ``mlbm_iterate`` call and a
 device->host read of its phase statistics, and the final density field
-copied out.
+copied out, over a job of max(K, 500) steps (``e2e.steps``).
 
 ``--impl reference`` runs the reference's own code: its time step compiled
 for the CPU (``oracle/_ref``, OpenMP over all host cores) on a bounded
@@ -64,6 +64,9 @@ def phys(n=200):
 
 
 PHYS = phys(200)
+# The end-to-end leg runs a job of at least this many steps (its one-time
+# upload and layout change are part of it), whatever --steps is.
+E2E_MIN_STEPS = 500
 BYTES_PER_FLUID = {"f32": 152, "f16": 76, "f64": 304}
 
 
@@ -453,7 +456,7 @@ def main():
             **phys(args.size), rho_shift=1.0),
             {"f32": capi.STORE_F32, "f16": capi.STORE_F16,
              "f64": capi.STORE_F64}[args.storage],
-            local, args.steps, dist, kernel_id)
+            local, max(args.steps, E2E_MIN_STEPS), dist, kernel_id)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline and args.size == 200:
