@@ -279,18 +279,33 @@ bool inject_now(const mlbm_lattice* lat, const StepArgs& a) {
 }
 }  // namespace
 
+namespace {
+// Launches into a stream that is being captured into a CUDA graph are plain:
+// the batched step's graphs with overlapped launches gave wrong states, so
+// the overlap is used in ordinary stream order only.
+bool stream_capturing(cudaStream_t stream) {
+  cudaStreamCaptureStatus st = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(stream, &st) != cudaSuccess) {
+    cudaGetLastError();  // a query refused during another capture: be plain
+    return true;
+  }
+  return st != cudaStreamCaptureStatusNone;
+}
+}  // namespace
+
 template <typename T>
 mlbm_status launch_compact_two_pass(mlbm_lattice* lat, const StepArgs& a,
                                     bool write_u, bool write_rho) {
   const bool inj = inject_now(lat, a);
   long long kb, ke;
   own_range(lat, kb, ke);
+  const bool overlap = !stream_capturing(lat->stream);
   if (lat->phase == 0) {
-    launch_c2_density<T, 0>(lat, a, write_rho, inj, kb, ke, true);
-    launch_c2_update<T, 0>(lat, a, write_u, inj, kb, ke, true);
+    launch_c2_density<T, 0>(lat, a, write_rho, inj, kb, ke, overlap);
+    launch_c2_update<T, 0>(lat, a, write_u, inj, kb, ke, overlap);
   } else {
-    launch_c2_density<T, 1>(lat, a, write_rho, inj, kb, ke, true);
-    launch_c2_update<T, 1>(lat, a, write_u, inj, kb, ke, true);
+    launch_c2_density<T, 1>(lat, a, write_rho, inj, kb, ke, overlap);
+    launch_c2_update<T, 1>(lat, a, write_u, inj, kb, ke, overlap);
   }
   const cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(e, "compact two-pass launch");
