@@ -130,3 +130,29 @@ def test_batch_domain_preempted_and_resumed(storage):
     other.iterate(0, 21)
     assert np.array_equal(b.lattice(ids[1]).field("f"), other.field("f"))
     b.close()
+
+
+@pytest.mark.parametrize("storage", [0, 1])
+def test_long_run_saved_resumed_and_reallocated(storage):
+    """Hundreds of steps, statistics read on the way, the lattice saved,
+    destroyed and resumed in a fresh lattice (whose buffers reuse the freed
+    memory), then hundreds more steps: bit-identical to the uninterrupted
+    run -- the serving flow on single lattices."""
+    from multiphase_lbm_b200 import capi
+    fluid, rho = sphere_case(SHAPE, seed=9, rmin=2.0, rmax=4.5, porosity=0.55,
+                             rho0=1.9, amp=0.05)
+    a = _lattice(capi, fluid, rho, storage, 0)
+    a.iterate(0, 400)
+    a.stats()
+    image = a.checkpoint(400)
+    a.close()
+    b = capi.Lattice(SHAPE, storage=storage)
+    assert b.restore(image) == 400
+    b.iterate(400, 300)
+    b.stats()
+    b.iterate(700, 300)
+    ref = _lattice(capi, fluid, rho, storage, 0)
+    ref.iterate(0, 1000)
+    assert np.array_equal(b.field("f"), ref.field("f"))
+    b.close()
+    ref.close()
