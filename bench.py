@@ -54,6 +54,13 @@ RHO_S = 0.182322  # -ln(1 - G_ads/G) for G_ads = -1, G = -6
 POSITIONS = os.path.join(ROOT, "multiphase_lbm_b200", "workloads",
                          "drainage_200_seed2024.positions")
 MIN_TIMED_S = 1.0  # timed blocks repeat until this much device time
+# The 64^3 periodic case (phase separation from rho 0.70 +- 0.01, the
+# reference's srand(1)/rand() stream): a second speed comparison against the
+# reference's CUDA build on identical geometry and boundaries.
+SHAPE_64 = (64, 64, 64)
+POSITIONS_64 = os.path.join(ROOT, "multiphase_lbm_b200", "workloads",
+                            "periodic_64_seed64.positions")
+RATE_64 = 0.02 / 0.70  # IniPerturbRate: rho0 (1 + rate (U - 0.5)), rho0 0.70
 
 
 def phys(n=200):
@@ -109,6 +116,33 @@ read_positions {POSITIONS}
 step_max 1000000000
 """
     path = os.path.join(folder, "bench_200.txt")
+    with open(path, "w") as fh:
+        fh.write(text)
+    return path
+
+
+def command_file_64(folder: str) -> str:
+    """The 64^3 periodic case as a reference command file."""
+    text = f"""! 64^3 periodic phase-separation case
+result_folder {folder}/RES64
+num_threads {len(os.sched_getaffinity(0))}
+statPeriod 1000000000
+lx 64
+ly 64
+lz 64
+rho0 0.70
+IniPerturbRate {RATE_64:.9g}
+G -6.0
+rhos {RHO_S}
+tau 1.0
+rhol_spinodal 0.2726
+rhog_spinodal 0.0484
+resize
+resolution 1
+read_positions {POSITIONS_64}
+step_max 1000000000
+"""
+    path = os.path.join(folder, "bench_64.txt")
     with open(path, "w") as fh:
         fh.write(text)
     return path
@@ -256,17 +290,21 @@ def cpu_reference_sample(budget_s=15.0, max_steps=200):
                       f"race-free two-sweep collision)"}
 
 
-def reference_cuda(folder: str, steps: int, warmup: int, device: int):
+def reference_cuda(folder: str, steps: int, warmup: int, device: int,
+                   n: int = 200):
     """The reference's CUDA build on this GPU: its unmodified
     multiphaselbm_iteration timed between CUDA events by
-    oracle/_ref/ref_cuda_timer_200x200x200, blocks of `steps` steps repeated
-    for about a second; median block."""
-    exe = os.path.join(ROOT, "oracle", "_ref", "ref_cuda_timer_200x200x200")
+    oracle/_ref/ref_cuda_timer_<n>x<n>x<n> (n = 200: the drainage packing;
+    n = 64: the periodic case), blocks of `steps` steps repeated for about a
+    second; median block."""
+    name = f"ref_cuda_timer_{n}x{n}x{n}"
+    exe = os.path.join(ROOT, "oracle", "_ref", name)
     if not os.path.exists(exe):
-        return {"unavailable": "oracle/_ref/ref_cuda_timer_200x200x200 not built"}
-    cmd = command_file(folder)
-    # ~3 ms per step: enough blocks for about a second of timed steps
-    repeats = max(3, int(MIN_TIMED_S / (0.003 * steps)) + 1)
+        return {"unavailable": f"oracle/_ref/{name} not built"}
+    cmd = command_file(folder) if n == 200 else command_file_64(folder)
+    # ~3 ms per step at 200^3: enough blocks for about a second of steps
+    est = 0.003 * (n / 200) ** 3 + 2e-5
+    repeats = max(3, int(MIN_TIMED_S / (est * steps)) + 1)
     with ClockSampler(device) as clocks:
         r = subprocess.run(
             ["bash", "-c", f"ulimit -s unlimited; exec {exe} {cmd} "
@@ -279,9 +317,10 @@ def reference_cuda(folder: str, steps: int, warmup: int, device: int):
                                f"{(r.stderr or r.stdout)[-200:]}"}
     ms = statistics.median(blocks)
     return {"ms_per_step": round(ms, 4),
-            "value": round(SHAPE[0] * SHAPE[1] * SHAPE[2] / (ms / 1e3) / 1e6, 2),
+            "value": round(n ** 3 / (ms / 1e3) / 1e6, 2),
             "unit": "MLUPS", "steps": steps, "blocks": len(blocks),
-            "boundaries": "periodic (the reference has no drainage boundary)",
+            "boundaries": "periodic (the reference has no drainage boundary)"
+                          if n == 200 else "periodic (as configured)",
             "clocks": clocks.summary()}
 
 
@@ -301,10 +340,12 @@ def run_reference_arm(args, rank, world):
         # each bench step is one lattice step; the sample stops after ~60 s
         n, dt = reference_cpu_steps(ref, args.warmup, args.steps, 60.0)
         mlups = fluid.size * n / dt / 1e6
-        cuda = None
+        cuda = cuda64 = None
         if not args.no_reference_cuda:
-            cuda = reference_cuda(folder, max(args.steps, 20), args.warmup,
-                                  int(os.environ.get("LOCAL_RANK", "0")))
+            dev = int(os.environ.get("LOCAL_RANK", "0"))
+            cuda = reference_cuda(folder, max(args.steps, 20), args.warmup, dev)
+            cuda64 = reference_cuda(folder, max(args.steps, 20), args.warmup,
+                                    dev, n=64)
     sample = (f"{n} of {args.steps} timed lattice steps (each bench step one "
               f"lattice step; stops after 60 s) of the 200^3 drainage case")
     line = {
@@ -322,6 +363,8 @@ def run_reference_arm(args, rank, world):
     }
     if cuda is not None:
         line["reference_cuda"] = cuda
+    if cuda64 is not None:
+        line["reference_cuda_64"] = cuda64
     print(json.dumps(line))
     return 0
 
@@ -377,6 +420,36 @@ def measure(capi, torch, fluid, rho, storage_name, args, local, dist,
     return ms / 1e3 / args.steps, blocks, clocks.summary(), kernel
 
 
+def measure_64(capi, torch, args, local):
+    """The default FP32 step on the 64^3 periodic case (the committed 64^3
+    positions file, rho 0.70 with the reference's srand(1)/rand()
+    perturbation, no inlet or outlet): median device time per step, in blocks
+    as long as the reference's CUDA timing uses."""
+    from multiphase_lbm_b200 import host
+    fluid, _, nsph = host.read_positions(POSITIONS_64, SHAPE_64)
+    rho = host.init_density(SHAPE_64, 0.70, RATE_64)
+    params = capi.default_params(G=-6.0, tau=1.0, rhos=RHO_S,
+                                 rhol_spinodal=0.2726, rhog_spinodal=0.0484,
+                                 rho_shift=1.0)
+    lat = capi.Lattice(SHAPE_64, storage=capi.STORE_F32, device=local)
+    lat.set_params(params)
+    lat.upload(fluid, rho)
+    lat.initialize()
+    steps = max(args.steps, 20)
+    lat.iterate(0, args.warmup)
+    torch.cuda.synchronize()
+    ms, blocks, _ = timed_blocks(lat, torch, args.warmup, steps, None,
+                                 min(args.min_time, 0.5))
+    kernel = KERNEL_INFO.get(lat.step_kernel, ("", str(lat.step_kernel)))[1]
+    lat.close()
+    per = ms / steps
+    return {"ms_per_step": round(per, 5),
+            "value": round(64 ** 3 / (per / 1e3) / 1e6, 2), "unit": "MLUPS",
+            "fluid_nodes": int(fluid.sum()), "spheres": int(nsph),
+            "steps": steps, "blocks": blocks, "kernel": kernel,
+            "boundaries": "periodic"}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -390,6 +463,8 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-fp16", action="store_true")
     ap.add_argument("--no-reference-cuda", action="store_true")
+    ap.add_argument("--no-64", action="store_true",
+                    help="skip the 64^3 periodic comparison case")
     ap.add_argument("--size", type=int, default=200,
                     help="lattice edge (profiling runs use a smaller case)")
     ap.add_argument("--kernel", default="auto",
@@ -461,6 +536,9 @@ def main():
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline and args.size == 200:
         cpu = cpu_reference_sample()
+    case64 = None
+    if world == 1 and not args.no_64 and args.size == 200:
+        case64 = measure_64(capi, torch, args, local)
 
     line = {
         "metric": "MLUPS", "value": round(mlups, 2), "unit": "MLUPS",
@@ -489,6 +567,8 @@ def main():
         line["e2e"] = e2e
     if cpu:
         line["cpu_baseline"] = cpu
+    if case64:
+        line["periodic_64"] = case64
     if rank == 0:
         print(json.dumps(line))
     if dist:

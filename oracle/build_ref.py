@@ -169,7 +169,7 @@ def build_dropin(sizes=None, force: bool = False) -> list[str]:
 # events: the reference's CUDA path measured on the B200 beside this library.
 # Not a parity oracle (its collision kernel reads neighbours another thread
 # may be writing, so its results are not deterministic).
-CUDA_SIZES = ["200x200x200"]
+CUDA_SIZES = ["64x64x64", "200x200x200"]
 
 
 def cuda_timer_path(size: str = "200x200x200") -> str:
