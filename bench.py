@@ -19,15 +19,20 @@ the median block is reported.  FP32 storage is the headline; the FP16-store
 form is timed in the same run (``fp16``).  ``e2e`` is the same metric
 through the C ABI with host buffers: geometry and initial density copied in
 from pinned host memory, then every step an ``mlbm_iterate`` call and a
-device->host read of its phase statistics, and the final density field
-copied out, over a job of max(K, 500) steps (``e2e.steps``).
+device->host read of its saturation and mass (the bulk statistics), and the
+final density field copied out, over a job of max(K, 500) steps
+(``e2e.steps``); ``e2e.with_full_stats_every_step`` reads every column of
+the phase statistics each step instead (the 18-neighbour boundary counts
+and the pressures included).
 
 ``--impl reference`` runs the reference's own code: its time step compiled
 for the CPU (``oracle/_ref``, OpenMP over all host cores) on a bounded
 sample of the same workload (the line's ``value``), and its CUDA build
 (``oracle/_ref/ref_cuda_timer_200x200x200``: the reference's unmodified
 kernels between CUDA events, periodic boundaries as the reference has no
-drainage boundary) on the same GPU (``reference_cuda``).  It loads nothing
+drainage boundary) on the same GPU (``reference_cuda``), and that build at
+64^3 on the periodic case (``reference_cuda_64``; this library's step on it
+is the ``periodic_64`` object of the other arm).  It loads nothing
 of this library.  ``--gpus N`` (under torchrun) runs N independent replicas,
 one per GPU (the single-domain step has no exchange to shard); value = all
 ranks' node updates / the slowest rank's time.
@@ -527,11 +532,15 @@ def main():
     # ---- end to end through the C ABI with host buffers --------------------
     e2e = None
     if not args.no_e2e:
-        e2e = run_e2e(capi, torch, fluid, rho, capi.default_params(
+        e2e_args = (capi, torch, fluid, rho, capi.default_params(
             **phys(args.size), rho_shift=1.0),
             {"f32": capi.STORE_F32, "f16": capi.STORE_F16,
              "f64": capi.STORE_F64}[args.storage],
             local, max(args.steps, E2E_MIN_STEPS), dist, kernel_id)
+        e2e = run_e2e(*e2e_args)
+        full = run_e2e(*e2e_args, full_stats=True)
+        e2e["with_full_stats_every_step"] = {
+            k: full[k] for k in ("value", "unit", "breakdown_ms")}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline and args.size == 200:
@@ -577,11 +586,13 @@ def main():
 
 
 def run_e2e(capi, torch, fluid, rho, params, storage, device, steps, dist,
-            kernel_id=None):
+            kernel_id=None, full_stats=False):
     """MLUPS through the public C ABI with host buffers (pinned).  Every
-    step's phase statistics are read back: enqueued without waiting
-    (mlbm_phase_stats_async) and read on the host one step later, while the
-    next step runs, so the GPU does not idle on the host's read."""
+    step's result is read back: its saturation and mass (the bulk
+    statistics, mlbm_bulk_stats_async; with full_stats every column of the
+    phase statistics, mlbm_phase_stats_async), enqueued without waiting and
+    read on the host one step later, while the next step runs, so the GPU
+    does not idle on the host's read."""
     fl_h = torch.from_numpy(fluid).pin_memory().numpy()
     rho_h = torch.from_numpy(rho).pin_memory().numpy()
     out_h = torch.empty(fluid.shape, dtype=torch.float32).pin_memory().numpy()
@@ -609,7 +620,8 @@ def run_e2e(capi, torch, fluid, rho, params, storage, device, steps, dist,
     sat = []
     for k in range(steps):
         lat.iterate(k, 1)
-        lat.stats_async(raw[k % 2])  # device->host read of the step's stats
+        # device->host read of the step's statistics
+        (lat.stats_async if full_stats else lat.bulk_stats_async)(raw[k % 2])
         done[k % 2].record()
         if k == 0:
             mark()  # the first step builds the fluid-only tables
@@ -636,7 +648,10 @@ def run_e2e(capi, torch, fluid, rho, params, storage, device, steps, dist,
     stats_bytes = 8 * capi.STATS_RAW_LEN
     assert len(sat) == steps
     return {"value": round(n * world * steps / dt / 1e6, 2), "unit": "MLUPS",
-            "steps": steps, "breakdown_ms": breakdown,
+            "steps": steps,
+            "per_step_read": "all phase statistics" if full_stats
+                             else "bulk statistics (saturation, mass, ...)",
+            "breakdown_ms": breakdown,
             "h2d_bytes_per_step": int((n + 4 * n) / steps),
             "d2h_bytes_per_step": int(stats_bytes + 4 * n / steps)}
 

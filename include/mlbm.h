@@ -264,6 +264,14 @@ mlbm_status mlbm_phase_stats(mlbm_lattice* lat, mlbm_stats* out);
 mlbm_status mlbm_phase_stats_async(mlbm_lattice* lat, double* raw);
 mlbm_status mlbm_stats_from_raw(mlbm_lattice* lat, const double* raw,
                                 mlbm_stats* out);
+/* The bulk columns of the same statistics, the same way (asynchronous, raw
+ * buffer of MLBM_STATS_RAW_LEN doubles, read with mlbm_stats_from_raw):
+ * n_fluid, n_liquid, n_vapour, mass, the liquid and vapour density sums and
+ * averages, saturation, min_rho and max_rho, each bit-identical to
+ * mlbm_phase_stats.  The boundary counts and everything made of pressures
+ * are not computed and read 0.  For a loop that reads the saturation and the
+ * mass of every step: it skips the 18-neighbour boundary test. */
+mlbm_status mlbm_bulk_stats_async(mlbm_lattice* lat, double* raw);
 /* Per-x-plane counts of fluid and liquid nodes (int64[nx] each).  Sync. */
 mlbm_status mlbm_plane_profile(mlbm_lattice* lat, int64_t* n_fluid_x,
                                int64_t* n_liquid_x);

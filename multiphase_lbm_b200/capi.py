@@ -125,6 +125,7 @@ SIGNATURES = [
     ("mlbm_halo_segments", C.c_int, [_VP, C.c_int32, C.c_int32, _VP, _VP,
                                      _VP]),
     ("mlbm_phase_stats_async", C.c_int, [_VP, _VP]),
+    ("mlbm_bulk_stats_async", C.c_int, [_VP, _VP]),
     ("mlbm_stats_from_raw", C.c_int, [_VP, _VP, C.POINTER(Stats)]),
     ("mlbm_slab_ring_create", C.c_int, [_VP, C.c_int32, C.POINTER(_VP)]),
     ("mlbm_slab_ring_exchange", C.c_int, [_VP, C.c_int32]),
@@ -345,6 +346,15 @@ class Lattice:
         if raw.dtype != np.float64 or raw.size < STATS_RAW_LEN:
             raise ValueError(f"raw must be float64[{STATS_RAW_LEN}]")
         check(lib().mlbm_phase_stats_async(self.h, _ptr(raw)))
+
+    def bulk_stats_async(self, raw: np.ndarray) -> None:
+        """As :meth:`stats_async` for the bulk columns only (counts, mass,
+        liquid/vapour density sums, saturation, min/max rho, bit-identical
+        to the full statistics; the boundary counts and the pressures read
+        0)."""
+        if raw.dtype != np.float64 or raw.size < STATS_RAW_LEN:
+            raise ValueError(f"raw must be float64[{STATS_RAW_LEN}]")
+        check(lib().mlbm_bulk_stats_async(self.h, _ptr(raw)))
 
     def stats_from_raw(self, raw: np.ndarray) -> dict:
         s = Stats()

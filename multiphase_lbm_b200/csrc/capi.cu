@@ -652,8 +652,9 @@ mlbm_status mlbm_download_field(mlbm_lattice* lat, int32_t field,
 namespace {
 
 // Enqueue the phase statistics reduction and the copy of its ST_COUNT + 1
-// doubles (the last one the device error flag) to host memory `h`.
-mlbm_status stats_enqueue(mlbm_lattice* lat, double* h) {
+// doubles (the last one the device error flag) to host memory `h`; `full`
+// false: the bulk columns only (stat_node<R, false>).
+mlbm_status stats_enqueue(mlbm_lattice* lat, double* h, bool full) {
   if (mlbm_status st = check_lat(lat)) return st;
   if (!h) return fail(MLBM_ERR_ARG, "null output");
   if (!lat->initialized) return fail(MLBM_ERR_STATE, "stats before initialize");
@@ -674,19 +675,23 @@ mlbm_status stats_enqueue(mlbm_lattice* lat, double* h) {
   // last block to finish writes the results).
   long long nblocks = (long long)grid.x * grid.y * grid.z, span = 0;
   if (fluid_list) {
-    if (lat->stats_wave <= 0) {
+    // the wave of each form from its own occupancy (the bulk form holds
+    // fewer registers)
+    int& wave = full ? lat->stats_wave : lat->stats_bulk_wave;
+    if (wave <= 0) {
       int per_sm = 0, nsm = 0;
       CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-                   &per_sm, k_stats_fluid<float>, kStatThreads, 0),
+                   &per_sm, full ? k_stats_fluid<float, true> : k_stats_fluid<float, false>,
+                   kStatThreads, 0),
                "stats occupancy");
       CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount,
                                       lat->device),
                "stats occupancy");
-      lat->stats_wave = std::max(1, per_sm * nsm);
+      wave = std::max(1, per_sm * nsm);
     }
     const long long rounds =
         std::max(1LL, (c.nfluid + kStatThreads - 1) / kStatThreads);
-    nblocks = std::min<long long>(lat->stats_wave, rounds);
+    nblocks = std::min<long long>(wave, rounds);
     span = (rounds + nblocks - 1) / nblocks * kStatThreads;
     nblocks = std::max(1LL, (c.nfluid + span - 1) / span);
   }
@@ -709,15 +714,18 @@ mlbm_status stats_enqueue(mlbm_lattice* lat, double* h) {
   sc.out = sc.records + (size_t)nblocks * ST_COUNT;
   double* fin = sc.out;
   if (fluid_list) {
-    k_stats_fluid<float><<<(unsigned)nblocks, kStatThreads, 0, lat->stream>>>(
+    auto kernel = full ? k_stats_fluid<float, true> : k_stats_fluid<float, false>;
+    kernel<<<(unsigned)nblocks, kStatThreads, 0, lat->stream>>>(
         static_cast<const float*>(lat->rho), c.cinfo, c.nfluid, span, lat->g,
         lat->phys, sc, lat->err);
   } else if (lat->storage == MLBM_STORE_F64) {
-    k_stats_partial<double><<<grid, dim3(32, 8), 0, lat->stream>>>(
+    auto kernel = full ? k_stats_partial<double, true> : k_stats_partial<double, false>;
+    kernel<<<grid, dim3(32, 8), 0, lat->stream>>>(
         static_cast<const double*>(lat->rho), lat->nbw, lat->g, lat->phys, sc,
         lat->err);
   } else {
-    k_stats_partial<float><<<grid, dim3(32, 8), 0, lat->stream>>>(
+    auto kernel = full ? k_stats_partial<float, true> : k_stats_partial<float, false>;
+    kernel<<<grid, dim3(32, 8), 0, lat->stream>>>(
         static_cast<const float*>(lat->rho), lat->nbw, lat->g, lat->phys, sc,
         lat->err);
   }
@@ -771,13 +779,17 @@ extern "C" {
 mlbm_status mlbm_phase_stats(mlbm_lattice* lat, mlbm_stats* out) {
   if (!out) return fail(MLBM_ERR_ARG, "null output");
   double h[ST_COUNT + 1];
-  if (mlbm_status st = stats_enqueue(lat, h)) return st;
+  if (mlbm_status st = stats_enqueue(lat, h, true)) return st;
   CUDA_TRY(cudaStreamSynchronize(lat->stream), "stats");
   return stats_convert(lat, h, out);
 }
 
 mlbm_status mlbm_phase_stats_async(mlbm_lattice* lat, double* raw) {
-  return stats_enqueue(lat, raw);
+  return stats_enqueue(lat, raw, true);
+}
+
+mlbm_status mlbm_bulk_stats_async(mlbm_lattice* lat, double* raw) {
+  return stats_enqueue(lat, raw, false);
 }
 
 mlbm_status mlbm_stats_from_raw(mlbm_lattice* lat, const double* raw,

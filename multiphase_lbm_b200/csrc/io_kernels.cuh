@@ -125,45 +125,59 @@ __device__ __forceinline__ double stat_identity(int k) {
 // The statistics of one fluid node folded into acc.  The liquid boundary
 // test reads the node's neighbour word (bit i: x - e_i is fluid) and the
 // density of every fluid neighbour, then takes the first neighbour
-// (i = 1..18) that is solid or not liquid, as calc_cluster does.
-template <typename R>
+// (i = 1..18) that is solid or not liquid, as calc_cluster does.  FULL =
+// false folds only the bulk columns (stat_bulk_column): no boundary test and
+// no pressure; those columns get the same operations in the same order
+// either way, so they come out bit-identical.
+template <typename R, bool FULL = true>
 __device__ __forceinline__ void stat_node(double (&acc)[ST_COUNT],
                                           const R* __restrict__ rho,
                                           const Geom& g, const Phys& p, int x,
                                           int y, int z, uint32_t nb, R r) {
   const R rhol = R(p.rhol_spinodal), rhog = R(p.rhog_spinodal);
-  const R pr = pressure_of<R>(p, r);
+  const R pr = FULL ? pressure_of<R>(p, r) : R(0);
   acc[ST_NF] += 1.0;
   acc[ST_MASS] += (double)r;
   if (r > rhol) {
     acc[ST_NL] += 1.0;
-    acc[ST_PL] += (double)pr;
+    if (FULL) acc[ST_PL] += (double)pr;
     acc[ST_RL] += (double)r;
-    Nbr a;
-    a.init(g, x, y, z);
-    // all 18 neighbour densities as independent loads (every periodic
-    // index lies inside the array, solid nodes included), then the masks:
-    // a load under each direction's branch would wait on the one before
-    R nr[Q];
+    if (FULL) {
+      Nbr a;
+      a.init(g, x, y, z);
+      // all 18 neighbour densities as independent loads (every periodic
+      // index lies inside the array, solid nodes included), then the masks:
+      // a load under each direction's branch would wait on the one before
+      R nr[Q];
 #pragma unroll
-    for (int i = 1; i < Q; ++i) nr[i] = __ldg(rho + a.idx(-ex(i), -ey(i), -ez(i)));
-    const uint32_t solid = ~nb & 0x7fffeu;  // directions 1..18
-    uint32_t low = 0u;
+      for (int i = 1; i < Q; ++i) nr[i] = __ldg(rho + a.idx(-ex(i), -ey(i), -ez(i)));
+      const uint32_t solid = ~nb & 0x7fffeu;  // directions 1..18
+      uint32_t low = 0u;
 #pragma unroll
-    for (int i = 1; i < Q; ++i) low |= (nr[i] < rhol ? 1u : 0u) << i;
-    const uint32_t other = low & nb & 0x7fffeu;
-    const uint32_t first = (solid | other) & (0u - (solid | other));
-    if (first & solid) acc[ST_NLS] += 1.0;
-    else if (first) acc[ST_NLV] += 1.0;
+      for (int i = 1; i < Q; ++i) low |= (nr[i] < rhol ? 1u : 0u) << i;
+      const uint32_t other = low & nb & 0x7fffeu;
+      const uint32_t first = (solid | other) & (0u - (solid | other));
+      if (first & solid) acc[ST_NLS] += 1.0;
+      else if (first) acc[ST_NLV] += 1.0;
+    }
   } else if (r < rhog) {
     acc[ST_NV] += 1.0;
-    acc[ST_PV] += (double)pr;
+    if (FULL) acc[ST_PV] += (double)pr;
     acc[ST_RV] += (double)r;
   }
   acc[ST_MINR] = fmin(acc[ST_MINR], (double)r);
   acc[ST_MAXR] = fmax(acc[ST_MAXR], (double)r);
-  acc[ST_MINP] = fmin(acc[ST_MINP], (double)pr);
-  acc[ST_MAXP] = fmax(acc[ST_MAXP], (double)pr);
+  if (FULL) {
+    acc[ST_MINP] = fmin(acc[ST_MINP], (double)pr);
+    acc[ST_MAXP] = fmax(acc[ST_MAXP], (double)pr);
+  }
+}
+
+// The columns that the bulk statistics (FULL = false) compute; the others
+// are written as 0.
+__host__ __device__ constexpr bool stat_bulk_column(int k) {
+  return k == ST_NF || k == ST_NL || k == ST_NV || k == ST_MASS ||
+         k == ST_RL || k == ST_RV || k == ST_MINR || k == ST_MAXR;
 }
 
 // Warp then block reduction of acc in a fixed order (deterministic); thread 0
@@ -208,7 +222,7 @@ struct StatScratch {
 // other SMs wrote them.  256 threads.
 __device__ __forceinline__ void stat_last_block(StatScratch s, unsigned nblocks,
                                                 const int* __restrict__ err,
-                                                int tid) {
+                                                int tid, bool full) {
   __shared__ bool last;
   __shared__ double sh[kStatThreads / 32][ST_COUNT];
   __threadfence();
@@ -239,7 +253,7 @@ __device__ __forceinline__ void stat_last_block(StatScratch s, unsigned nblocks,
   if (tid < ST_COUNT) {
     double r = sh[0][tid];
     for (int w = 1; w < kStatThreads / 32; ++w) r = stat_op(tid, r, sh[w][tid]);
-    s.out[tid] = r;
+    s.out[tid] = full || stat_bulk_column(tid) ? r : 0.0;  // not computed: 0
   }
   if (tid == 0) {
     s.out[ST_COUNT] = err ? (double)*err : 0.0;
@@ -249,7 +263,7 @@ __device__ __forceinline__ void stat_last_block(StatScratch s, unsigned nblocks,
 
 // Dense form: one block per 32 x 8 nodes of an (x, y) plane and kStatZ
 // planes; each thread folds its column of nodes, z ascending.
-template <typename R>
+template <typename R, bool FULL = true>
 __global__ void __launch_bounds__(kStatThreads)
     k_stats_partial(const R* __restrict__ rho, const uint32_t* __restrict__ nbw,
                     Geom g, Phys p, StatScratch sc, const int* __restrict__ err) {
@@ -279,14 +293,15 @@ __global__ void __launch_bounds__(kStatThreads)
       }
 #pragma unroll
       for (int j = 0; j < U; ++j)
-        if (nbv[j] & NB_SELF) stat_node<R>(acc, rho, g, p, x, y, zb + j, nbv[j], rv[j]);
+        if (nbv[j] & NB_SELF)
+          stat_node<R, FULL>(acc, rho, g, p, x, y, zb + j, nbv[j], rv[j]);
     }
   }
   const long long blk =
       blockIdx.x + (long long)gridDim.x * (blockIdx.y + (long long)gridDim.y * blockIdx.z);
   const int tid = threadIdx.y * 32 + threadIdx.x;
   stat_block_reduce(acc, tid, sc.records + blk * ST_COUNT);
-  stat_last_block(sc, gridDim.x * gridDim.y * gridDim.z, err, tid);
+  stat_last_block(sc, gridDim.x * gridDim.y * gridDim.z, err, tid, FULL);
 }
 
 // Fluid-list form, for a lattice held in the fluid-only layout: the threads
@@ -295,7 +310,7 @@ __global__ void __launch_bounds__(kStatThreads)
 // it); block b folds slots [b * span, (b + 1) * span) and thread t takes
 // slots t, t + 256, ... of them, ascending -- a fixed assignment, so the
 // sums do not depend on scheduling.
-template <typename R>
+template <typename R, bool FULL = true>
 __global__ void __launch_bounds__(kStatThreads)
     k_stats_fluid(const R* __restrict__ rho, const uint2* __restrict__ cinfo,
                   long long nslots, long long span, Geom g, Phys p,
@@ -326,12 +341,12 @@ __global__ void __launch_bounds__(kStatThreads)
 #pragma unroll
     for (int j = 0; j < U; ++j)
       if (ci[j].x & NB_SELF)
-        stat_node<R>(acc, rho, g, p, (int)(ci[j].y & 2047u),
+        stat_node<R, FULL>(acc, rho, g, p, (int)(ci[j].y & 2047u),
                      (int)((ci[j].y >> 11) & 2047u), (int)(ci[j].y >> 22),
                      ci[j].x, rv[j]);
   }
   stat_block_reduce(acc, threadIdx.x, sc.records + (long long)blockIdx.x * ST_COUNT);
-  stat_last_block(sc, gridDim.x, err, threadIdx.x);
+  stat_last_block(sc, gridDim.x, err, threadIdx.x, FULL);
 }
 
 // Per-x-plane fluid / liquid node counts (integer atomics: deterministic).

@@ -50,6 +50,7 @@ def test_statistics_entry_points_refuse_bad_arguments():
     L = capi.lib()
     raw = np.zeros(capi.STATS_RAW_LEN, np.float64)
     _refused(L.mlbm_phase_stats_async(None, raw.ctypes.data), "null lattice")
+    _refused(L.mlbm_bulk_stats_async(None, raw.ctypes.data), "null lattice")
     s = capi.Stats()
     _refused(L.mlbm_stats_from_raw(None, raw.ctypes.data, C.byref(s)),
              "null lattice")

@@ -223,6 +223,48 @@ def test_async_stats_equal_sync_stats_every_step():
     assert got == want
 
 
+BULK_KEYS = ("n_fluid", "n_liquid", "n_vapour", "mass", "sum_rho_liquid",
+             "sum_rho_vapour", "saturation", "avg_rho_liquid",
+             "avg_rho_vapour", "min_rho", "max_rho")
+
+
+@pytest.mark.parametrize("storage,kernel", [(0, 0), (1, 0), (2, 0), (0, 2)],
+                         ids=["f32-auto", "f16-auto", "f64", "f32-dense"])
+def test_bulk_stats_equal_the_full_statistics(storage, kernel):
+    """mlbm_bulk_stats_async: its columns are bit-identical to
+    mlbm_phase_stats on the same state (the fluid-list walk of the compact
+    layout, the dense walk in FP32 and FP64), the columns it skips read 0,
+    and a second call gives the same result."""
+    import torch
+
+    from multiphase_lbm_b200 import capi
+    shape = (48, 40, 32)
+    fluid, _ = sphere_case(shape, seed=8)
+    # liquid, vapour and in-between nodes side by side in the initial state
+    # (one step of streaming mixes them: after it no node is vapour); then
+    # after one and two steps, the two AA phases
+    rho = np.random.default_rng(8).uniform(0.02, 0.9, shape).astype(np.float32)
+    lat, _ = _pair(shape, fluid, rho, storage=storage, kernel=kernel,
+                   **SC_PARAMS)
+    raw = torch.zeros(capi.STATS_RAW_LEN, dtype=torch.float64).pin_memory().numpy()
+    for step in range(3):
+        if step:
+            lat.iterate(step, 1)
+        lat.bulk_stats_async(raw)
+        lat.synchronize()
+        bulk = lat.stats_from_raw(raw)
+        full = lat.stats()
+        lat.bulk_stats_async(raw)
+        lat.synchronize()
+        assert lat.stats_from_raw(raw) == bulk
+        assert full["n_liquid"] > 0 and (step or full["n_vapour"] > 0)
+        for key in BULK_KEYS:
+            assert bulk[key] == full[key], key
+        for key in set(full) - set(BULK_KEYS):
+            assert bulk[key] == 0, key
+    lat.close()
+
+
 def test_mass_conservation_periodic_full_size():
     """Periodic, no injection: total fluid mass is conserved (BGK and
     bounce-back conserve mass); FP64 reduction, 200^3, 20 steps."""
