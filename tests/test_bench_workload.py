@@ -10,6 +10,9 @@
   slabs included, over the first steps of both AA phases -- so the GPU
   parity tests at this size, which compare against the oracle, compare
   against the reference.
+* The 64^3 periodic comparison case reads the same geometry and initial
+  density in both arms (the reference's parser on the command file its CUDA
+  build is timed with; this library's readers on the same positions file).
 """
 import os
 import sys
@@ -60,3 +63,23 @@ def test_oracle_bit_exact_with_reference_at_bench_size(tmp_path):
         for field in ("rho", "f"):
             a, b = ref.get(field), port.get(field)
             assert np.array_equal(a, b), f"step {step}: {field}"
+
+
+def test_periodic_64_case_same_geometry_and_density_in_both_arms(tmp_path):
+    """The 64^3 periodic comparison case: the command file the reference arm
+    gives the reference's CUDA build, read by the reference's own parser,
+    yields the mask and initial density (its srand(1)/rand() perturbation)
+    that this library's arm builds from the same positions file."""
+    from multiphase_lbm_b200 import host
+    shape = bench.SHAPE_64
+    if shape not in oracle.reference_sizes():
+        pytest.skip("oracle/_ref has no 64^3 build")
+    ref = oracle.Reference(shape)
+    r_rho, r_fl, _, info = ref.driver_read(bench.command_file_64(str(tmp_path)))
+    fluid, _, n = host.read_positions(bench.POSITIONS_64, shape)
+    rho = host.init_density(shape, 0.70, bench.RATE_64)
+    assert n == int(info["solid_count"]) == 276
+    assert np.array_equal(r_fl, fluid) and int(fluid.sum()) == 131062
+    assert np.array_equal(r_rho[fluid == 1], rho[fluid == 1])
+    gen, spheres = host.generate_packing(shape, 2.5, 7.5, 0.50, 64)
+    assert len(spheres) == n and np.array_equal(gen, fluid)
