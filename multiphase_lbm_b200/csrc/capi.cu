@@ -675,23 +675,22 @@ mlbm_status stats_enqueue(mlbm_lattice* lat, double* h, bool full) {
   // last block to finish writes the results).
   long long nblocks = (long long)grid.x * grid.y * grid.z, span = 0;
   if (fluid_list) {
-    // the wave of each form from its own occupancy (the bulk form holds
-    // fewer registers)
-    int& wave = full ? lat->stats_wave : lat->stats_bulk_wave;
-    if (wave <= 0) {
+    // Both forms use the full form's wave: the spans, and with them the
+    // order of every sum, are then the same, so the bulk columns come out
+    // bit-identical.
+    if (lat->stats_wave <= 0) {
       int per_sm = 0, nsm = 0;
       CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-                   &per_sm, full ? k_stats_fluid<float, true> : k_stats_fluid<float, false>,
-                   kStatThreads, 0),
+                   &per_sm, k_stats_fluid<float, true>, kStatThreads, 0),
                "stats occupancy");
       CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount,
                                       lat->device),
                "stats occupancy");
-      wave = std::max(1, per_sm * nsm);
+      lat->stats_wave = std::max(1, per_sm * nsm);
     }
     const long long rounds =
         std::max(1LL, (c.nfluid + kStatThreads - 1) / kStatThreads);
-    nblocks = std::min<long long>(wave, rounds);
+    nblocks = std::min<long long>(lat->stats_wave, rounds);
     span = (rounds + nblocks - 1) / nblocks * kStatThreads;
     nblocks = std::max(1LL, (c.nfluid + span - 1) / span);
   }

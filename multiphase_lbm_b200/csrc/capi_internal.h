@@ -60,7 +60,6 @@ struct mlbm_lattice {
   double* stats_scratch = nullptr;
   size_t stats_scratch_bytes = 0;
   int stats_wave = 0;           // resident blocks of the statistics kernel
-  int stats_bulk_wave = 0;      // the same for its bulk form
 
   // update pass: z-march tiles and the TMA descriptor of the psi tensor
   mlbm::ZMarch zm{};

@@ -234,11 +234,13 @@ def test_bulk_stats_equal_the_full_statistics(storage, kernel):
     """mlbm_bulk_stats_async: its columns are bit-identical to
     mlbm_phase_stats on the same state (the fluid-list walk of the compact
     layout, the dense walk in FP32 and FP64), the columns it skips read 0,
-    and a second call gives the same result."""
+    and a second call gives the same result.  The lattice has more fluid
+    nodes than one wave of the fluid-list walk's blocks covers (~114 k on a
+    B200), so its blocks take spans of several rounds."""
     import torch
 
     from multiphase_lbm_b200 import capi
-    shape = (48, 40, 32)
+    shape = (96, 80, 64)
     fluid, _ = sphere_case(shape, seed=8)
     # liquid, vapour and in-between nodes side by side in the initial state
     # (one step of streaming mixes them: after it no node is vapour); then
